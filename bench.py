@@ -1,0 +1,385 @@
+#!/usr/bin/env python
+"""Benchmark of the normal-estimation path: normals/s end to end at k=16.
+
+Workload (default): 2M points sampled on a synthetic scene (32 spheres of
+radius 0.02-0.2 and 8 planes clipped to the unit cube, area-weighted, Gaussian
+jitter 0.002 along the normal), 63-bit Morton codes, k=16, exact kNN.
+
+A step is one pass of the path over one cloud: build (bbox, encode, sort,
+dedup, radix tree, octree) followed by normals for every unique point.
+  value  device-resident: inputs already in HBM, normals written to HBM
+  e2e    through the C ABI with host buffers: pinned host x/y/z copied in and
+         the normals copied out inside the timed region
+Both are timed with CUDA events on the stream the library runs on, L2 flushed
+(256 MB write) before every timed step, max over ranks.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+With N > 1 (torchrun) every rank runs an independent replica on its own cloud
+(weak scaling; the path has no exchange step). `--impl reference` times the
+reference pipeline restated on the host cores (rank 0 only), and the
+reference's own CUDA build when it was compiled (oracle/_ref).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "normals/sec end-to-end @k=16: learned-radius vs plain GPU, exact kNN, ≤1e-3 rad"
+
+
+def _workloads():
+    from shapeextraction_b200 import synth
+
+    return {
+        "scene_2M_k16": dict(gen=lambda s: synth.scene(2_000_000, s), k=16, code_bits=63,
+                             desc="2M points on 32 spheres + 8 planes, jitter 0.002, 63-bit codes, k=16"),
+        "precision_20M_k16": dict(gen=lambda s: synth.precision_mix(20_000_000, s), k=16, code_bits=63,
+                                  desc="20M points precision mix, 63-bit codes, k=16"),
+        "gmm_50M_k16": dict(gen=lambda s: synth.gaussian_mixture(50_000_000, s), k=16, code_bits=63,
+                            desc="50M points Gaussian mixture + surfaces, 63-bit codes, k=16"),
+        "cube_100k_k10": dict(gen=lambda s: synth.uniform_cube(100_000, s), k=10, code_bits=30,
+                              desc="100k uniform points, 30-bit codes, k=10"),
+    }
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _traffic_from_profiles(workload):
+    """Per-launch DRAM bytes of the fused kNN kernel from a committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", f"knn_normals_{workload}.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.strip().startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            f = [c.strip() for c in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((float(f[1]), float(f[2]), f[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i in range(4) if r[i].lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_ours(a):
+    import torch
+    import torch.distributed as dist
+
+    from shapeextraction_b200 import Context
+
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    wl = _workloads()[a.workload]
+    k = wl["k"]
+    x, y, z = wl["gen"](a.seed + rank)
+    n = x.size
+    hx, hy, hz = (torch.from_numpy(v).pin_memory() for v in (x, y, z))
+    dx, dy, dz = (v.cuda() for v in (hx, hy, hz))
+    stream = torch.cuda.current_stream()
+    ctx = Context(code_bits=wl["code_bits"], device=local, stream=stream.cuda_stream,
+                  eigengap_fp64=a.eigengap, leaf_bucket=a.bucket)
+    u = ctx.build(dx, dy, dz)["n_points"]
+    out_dev = torch.empty((u, 3), dtype=torch.float32, device="cuda")
+    out_host = torch.empty((u, 3), dtype=torch.float32).pin_memory()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
+
+    def step_device():
+        ctx.build(dx, dy, dz)
+        ctx.normals(k, out=out_dev)
+
+    def step_e2e():
+        ctx.build(hx, hy, hz)
+        ctx.normals(k, out=out_host)
+
+    def timed(step, steps, prof=None):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for i in range(steps):
+            flush.fill_(float(i))
+            ev[i][0].record(stream)
+            step()
+            ev[i][1].record(stream)
+            if prof is not None:
+                prof.append(ctx.profile())
+        torch.cuda.synchronize()
+        return sum(s.elapsed_time(e) for s, e in ev)
+
+    for _ in range(a.warmup):
+        step_device()
+        step_e2e()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = Clocks(local)
+    clk.start()
+    profs = []
+    ms_dev = timed(step_device, a.steps, profs)
+    stats = ctx.stats()
+    ms_e2e = timed(step_e2e, a.steps)
+    clocks = clk.stop()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+        t = torch.tensor([ms_dev, ms_e2e], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_dev, ms_e2e = float(t[0]), float(t[1])
+        tu = torch.tensor([u], dtype=torch.int64, device="cuda")
+        dist.all_reduce(tu, op=dist.ReduceOp.SUM)
+        u_all = int(tu[0])
+    else:
+        u_all = u
+
+    # dominant kernel: the fused kNN + normals kernel
+    q_ms = statistics.mean(p["query_ms"] for p in profs)
+    build_ms = {s: statistics.mean(p["build_ms"][s] for p in profs) for s in profs[0]["build_ms"]}
+    launches = sum(p["build_launches"] + p["query_launches"] for p in profs)
+    m = ctx.info()["n_octree"]
+    alg_bytes = 36 * u + 32 * m  # query + neighbour points read once, octree nodes read once, normals written
+    peak, peak_kind = _peaks()
+    achieved = alg_bytes / (q_ms * 1e-3) / 1e9
+    traffic = _traffic_from_profiles(a.workload)
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cpu = cpu_baseline(a.workload, a.seed, a.cpu_sample)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": u_all * a.steps / (ms_dev * 1e-3),
+            "unit": "normals/s",
+            "n_gpus": world,
+            "steps": a.steps,
+            "warmup": a.warmup,
+            "ms_per_step": ms_dev / a.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic (seeded generator, no dataset)",
+            "config": {"workload": a.workload, "desc": wl["desc"], "n_points": int(n), "unique_points": int(u),
+                       "k": k, "code_bits": wl["code_bits"], "octree_nodes": int(m),
+                       "l2": "flushed by a 256 MB device write before every timed step",
+                       "parallelism": f"{world} independent replica(s), one cloud per GPU",
+                       "leaf_bucket": a.bucket, "eigengap_fp64": a.eigengap},
+            "e2e": {"value": u_all * a.steps / (ms_e2e * 1e-3), "unit": "normals/s",
+                    "ms_per_step": ms_e2e / a.steps, "h2d_bytes_per_step": int(12 * n),
+                    "d2h_bytes_per_step": int(12 * u)},
+            "roofline": {"bound": "hbm", "kernel": "k_knn (fused kNN + covariance + eigensolve + orientation)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_source": peak_kind, "traffic": traffic, "alg_bytes_per_launch": int(alg_bytes),
+                         "launch_ms": q_ms},
+            "stages_ms": {**build_ms, "knn_normals": q_ms},
+            "gpu_launches": int(launches),
+            "fp64_solves_last_step": stats["fp64_solves"],
+            "nodes_visited_per_query": stats["nodes_visited"] / max(u, 1) * 32,
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def cpu_baseline(workload, seed, sample):
+    """The reference pipeline restated on the host cores, on a bounded sample."""
+    from oracle import oracle as O
+
+    wl = _workloads()[workload]
+    from shapeextraction_b200 import synth
+
+    if workload.startswith("cube"):
+        x, y, z = synth.uniform_cube(min(sample, 100_000), seed)
+    else:
+        x, y, z = synth.scene(sample, seed)
+    O.pipeline_reference(x[:1000], y[:1000], z[:1000], wl["k"])  # warm the library
+    t = time.perf_counter()
+    u, _ = O.pipeline_reference(x, y, z, wl["k"])
+    dt = time.perf_counter() - t
+    return {"value": u / dt, "unit": "normals/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"{x.size} points of the same scene generator, k={wl['k']}: reference pipeline restated on "
+                      "the host (bit-exact build, the reference's approximate octree search, FP32 covariance, "
+                      "FP64 Jacobi), OpenMP on all cores", "seconds": dt}
+
+
+def reference_cuda(workload, seed, reps=3):
+    """The reference's own CUDA build (oracle/_ref/refdriver) on the full workload."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "refdriver")
+    if not os.path.exists(exe):
+        return {"unavailable": "oracle/_ref/refdriver not built"}
+    from oracle import oracle as O
+    from shapeextraction_b200 import synth
+
+    wl = _workloads()[workload]
+    x, y, z = wl["gen"](seed)
+    a = O.build_stages(x, y, z, 63, root_compat=True)["radix"]
+    b = O.build_stages(x, y, z, 63, root_compat=False)["radix"]
+    if not all(np.array_equal(a[key][:1], b[key][:1]) for key in ("leftChild", "prefixN", "hasLeafLeft", "hasLeafRight")):
+        return {"unavailable": "the reference's root range breaks this cloud's tree (it would read unset parents)"}
+    with tempfile.TemporaryDirectory() as tmp:
+        f = os.path.join(tmp, "cloud.bin")
+        synth.to_cloud_file(f, x, y, z)
+        try:
+            r = subprocess.run([exe, "bench", f, str(wl["k"]), "1", str(reps)], capture_output=True, text=True,
+                               timeout=900)
+        except subprocess.TimeoutExpired:
+            return {"unavailable": "reference CUDA build exceeded 900 s"}
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("REFJSON ")]
+    if r.returncode != 0 or not lines:
+        return {"unavailable": f"refdriver exit {r.returncode}: {r.stderr[-300:]}"}
+    d = json.loads(lines[-1][8:])
+    ms = statistics.median(d["ms"])
+    return {"value": d["u"] / (ms * 1e-3), "unit": "normals/s", "ms": d["ms"], "u": d["u"],
+            "span": "host PointCloud in -> RadixTree ctor -> Octree ctor -> estimateNormals<k> -> host normals",
+            "build": "unmodified reference sources, nvcc 12.9 -O3 -DNDEBUG sm_100a (oracle/build_ref.sh)",
+            "cuda_error": d.get("cuda_error")}
+
+
+def run_reference(a):
+    world, rank, local = _dist()
+    if rank != 0:
+        return
+    wl = _workloads()[a.workload]
+    from oracle import oracle as O
+    from shapeextraction_b200 import synth
+
+    if a.workload.startswith("cube"):
+        x, y, z = synth.uniform_cube(min(a.cpu_sample, 100_000), a.seed)
+    else:
+        x, y, z = synth.scene(a.cpu_sample, a.seed)
+    for _ in range(a.warmup):
+        O.pipeline_reference(x, y, z, wl["k"])
+    times = []
+    u = 0
+    for _ in range(a.steps):
+        t = time.perf_counter()
+        u, _ = O.pipeline_reference(x, y, z, wl["k"])
+        times.append(time.perf_counter() - t)
+    tot = sum(times)
+    value = u * a.steps / tot
+    sample = (f"{x.size} points of the same scene generator per step, k={wl['k']}: reference pipeline restated on "
+              "the host (bit-exact build, the reference's approximate octree search, FP32 covariance, FP64 Jacobi)")
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": "normals/s",
+        "n_gpus": world,
+        "steps": a.steps,
+        "warmup": a.warmup,
+        "ms_per_step": tot / a.steps * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded generator, no dataset)",
+        "config": {"workload": a.workload, "desc": wl["desc"], "k": wl["k"], "code_bits": wl["code_bits"]},
+        "cpu_baseline": {"value": value, "unit": "normals/s", "cores": os.cpu_count(), "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "normals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    if not a.no_reference_cuda:
+        line["reference_cuda_build"] = reference_cuda(a.workload, a.seed)
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="scene_2M_k16")
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--bucket", type=int, default=16)
+    ap.add_argument("--eigengap", type=float, default=1e-4)
+    ap.add_argument("--cpu-sample", type=int, default=200_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-cuda", action="store_true")
+    a = ap.parse_args()
+    if a.warmup < 3:
+        a.warmup = 3
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,172 @@
+/*
+ * shapex.h -- C ABI of the B200-native normal-estimation path.
+ *
+ * Drop-in boundary for the reference's C++ entry points (Wehrdo/ShapeExtraction,
+ * paths relative to its project root). Every entry point cites the reference
+ * interface it replaces. Plain pointers and sizes only; every call returns an
+ * se_status. A context owns its device memory and one CUDA stream; use one
+ * context per host thread.
+ *
+ * Memory arguments (`mem`): SE_MEM_HOST means the pointer is host memory (the
+ * call copies through the context's stream and returns after the copy ends);
+ * SE_MEM_DEVICE means device memory on the context's device (the call only
+ * enqueues work, except where stated).
+ */
+#ifndef SHAPEX_H
+#define SHAPEX_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SE_ABI_VERSION 1
+
+typedef enum se_status {
+    SE_OK = 0,
+    SE_ERR_INVALID_ARG = 1,   /* bad pointer, size, k or option */
+    SE_ERR_CUDA = 2,          /* a CUDA runtime call failed (text in se_last_error) */
+    SE_ERR_OOM = 3,           /* device allocation failed */
+    SE_ERR_NOT_BUILT = 4,     /* query before a successful se_build */
+    SE_ERR_NONFINITE = 5,     /* NaN or Inf among the input coordinates */
+    SE_ERR_SEARCH_LIMIT = 6,  /* a kNN traversal hit its iteration or stack cap */
+    SE_ERR_DEVICE_CHECK = 7,  /* a kernel's own bounds check fired */
+    SE_ERR_SYNC_TIMEOUT = 8,  /* a cross-block wait (scan look-back) gave up */
+    SE_ERR_UNSUPPORTED = 9    /* e.g. a k outside {1..32}, or no sm_100 device */
+} se_status;
+
+typedef enum se_mem { SE_MEM_HOST = 0, SE_MEM_DEVICE = 1 } se_mem;
+
+typedef struct se_ctx se_ctx;
+
+/* Options. se_options_init fills the reference's behaviour. */
+typedef struct se_options {
+    int32_t code_bits;     /* 63 (21 bits/axis, src/MortonUtils.hpp:10) or 30 (10 bits/axis) */
+    int32_t root_compat;   /* 1: radix root covers [0, u-2] as src/RadixTree.cu:128-130
+                              with N = u-1 (src/RadixTree.cu:353-362); 0: full [0, u-1] */
+    int32_t build_octree;  /* 1: build the OTNode array (OT::Octree); 0: radix tree only */
+    float viewpoint[3];    /* orientation viewpoint, src/NormalEstimation.hpp:318-319 */
+    float eigengap_fp64;   /* relative eigengap (l1-l0)/l2 below which the 3x3
+                              eigensolve is redone in FP64 on the GPU */
+    int32_t leaf_bucket;   /* kNN bucket size: subtrees of <= this many points are
+                              scanned directly (1..32; 0 = default) */
+    int32_t device;        /* CUDA device ordinal */
+    void* stream;          /* cudaStream_t to use; NULL: the context creates one */
+    int32_t reserved[8];
+} se_options;
+
+/* Sizes after se_build (RT::RadixTree / OT::Octree public fields). */
+typedef struct se_info {
+    int64_t n_input;   /* points given to se_build */
+    int64_t n_points;  /* unique codes u (RadixTree::n_pts after dedup, src/RadixTree.cu:290) */
+    int64_t n_radix;   /* u-1 internal nodes (RadixTree::n_nodes, src/RadixTree.cu:353) */
+    int64_t n_octree;  /* octree nodes (Octree::n_nodes, src/Octree.cu:247) */
+    float min_coord;   /* RadixTree::min_coord, src/RadixTree.cu:241 */
+    float max_coord;   /* RadixTree::max_coord, src/RadixTree.cu:240 */
+    int32_t code_bits;
+    int32_t root_level; /* prefixN[0] / 3, src/Octree.cu:258 */
+} se_info;
+
+/* Byte-compatible with OT::OTNode, src/Octree.hpp:19-36 (56 bytes). */
+typedef struct se_otnode {
+    int32_t children[8];
+    float corner[3];
+    float cell_size;
+    int32_t child_node_mask;
+    int32_t child_leaf_mask;
+} se_otnode;
+
+/* Device pointers owned by the context (valid until the next se_build or
+ * se_destroy). Layouts: codes u64[u]; points float[3u] (AoS `Point`,
+ * src/PointCloud.hpp:21-36); octree se_otnode[n_octree]; radix arrays as
+ * RT::Nodes (src/RadixTree.hpp:17-34). */
+typedef struct se_device_views {
+    const uint64_t* codes;
+    const float* points;
+    const se_otnode* octree;
+    const int32_t* left_child;
+    const int32_t* parent;
+    const uint8_t* prefix_n;
+    const uint8_t* has_leaf_left;
+    const uint8_t* has_leaf_right;
+} se_device_views;
+
+int se_options_init(se_options* opt);
+const char* se_status_string(int status);
+int se_abi_version(void);
+
+/* Context lifetime. Replaces the implicit global state of the reference
+ * (default stream, per-call cudaMallocManaged). */
+int se_create(se_ctx** ctx, const se_options* opt);
+int se_destroy(se_ctx* ctx);
+const char* se_last_error(const se_ctx* ctx);
+
+/* Replaces RT::RadixTree::RadixTree(const PointCloud<float>&)
+ * (src/RadixTree.hpp:38, src/RadixTree.cu:305-382) followed by
+ * OT::Octree::Octree(const RT::RadixTree&) (src/Octree.hpp:95,
+ * src/Octree.cu:213-319): bbox, Morton encode, sort, dedup, Karras radix tree,
+ * octree, decode. x, y, z are the SoA coordinate arrays of PointCloud<float>
+ * (src/PointCloud.hpp:105-122). Returns after the build has finished. */
+int se_build(se_ctx* ctx, const float* x, const float* y, const float* z, int64_t n, int mem);
+
+/* RadixTree::n_pts/n_nodes/min_coord/max_coord, Octree::n_pts/n_nodes. */
+int se_get_info(const se_ctx* ctx, se_info* info);
+/* Device pointers to the built arrays (RadixTree::d_tree, Octree::u_nodes, Octree::u_points). */
+int se_get_device_views(const se_ctx* ctx, se_device_views* views);
+
+/* Copies of the build stages for parity checks. */
+/* RT::Nodes::mortonCode after dedup (src/RadixTree.cu:294-296): u codes, ascending. */
+int se_get_codes(se_ctx* ctx, uint64_t* out, int mem);
+/* RT::Nodes arrays, src/RadixTree.cu:344-362: n_radix entries each; parent has
+ * u entries (entries never written by the tree, e.g. parent[0], are 0). */
+int se_get_radix(se_ctx* ctx, int32_t* left_child, int32_t* parent, uint8_t* prefix_n,
+                 uint8_t* has_leaf_left, uint8_t* has_leaf_right, int mem);
+/* Octree::u_nodes, src/Octree.cu:250-282: n_octree nodes. */
+int se_get_octree(se_ctx* ctx, se_otnode* out, int mem);
+/* Octree::u_points / h_points, src/Octree.cu:305-318: u points, AoS xyz. */
+int se_get_points(se_ctx* ctx, float* out_xyz, int mem);
+
+/* Replaces Octree::deviceKnnSearch<k>(d_query, d_nn, N, eps) (src/Octree.hpp:106-107,
+ * 199-212) with the tree's own points [start, start+count) as queries, as
+ * NormalEstimation::estimateNormals does (src/NormalEstimation.hpp:204,211).
+ * Exact kNN, rows ascending by (squared distance, index); out_idx count*k
+ * int32, out_d2 (optional, may be NULL) count*k float. 1 <= k <= 32. */
+int se_knn_self(se_ctx* ctx, int k, int64_t start, int64_t count, int32_t* out_idx, float* out_d2, int mem);
+
+/* Replaces Octree::knnSearch<k>(points, eps) (src/Octree.hpp:102-103, 214-242)
+ * for arbitrary query points (AoS xyz, n_queries of them), with the
+ * reference's N/eps argument swap (src/Octree.hpp:232) not reproduced. */
+int se_knn(se_ctx* ctx, int k, const float* queries_xyz, int64_t n_queries, int32_t* out_idx, float* out_d2,
+           int mem);
+
+/* Replaces NormalEstimation::estimateNormals<k>(octree, start_idx, n)
+ * (src/NormalEstimation.hpp:16-19, 196-335): exact kNN, covariance, 3x3
+ * symmetric eigensolve, orientation towards the viewpoint, fused in one
+ * kernel. out_xyz: count normals, AoS xyz (std::vector<Point> layout). */
+int se_normals(se_ctx* ctx, int k, int64_t start, int64_t count, float* out_xyz, int mem);
+
+/* Counters of the last se_normals/se_knn call: queries whose eigensolve took
+ * the FP64 path, and total tree nodes visited (diagnostics). */
+int se_get_stats(const se_ctx* ctx, int64_t* fp64_solves, int64_t* nodes_visited);
+
+/* Device timings of the last se_build and query call, from CUDA events
+ * recorded on the context's stream around each stage, and the number of
+ * kernels each call launched. build_ms: bbox, encode (+ sort histograms),
+ * radix sort, dedup + decode, radix tree, search boxes, octree, total. */
+typedef struct se_profile {
+    float build_ms[8];
+    float query_ms;
+    int32_t build_launches;
+    int32_t query_launches;
+} se_profile;
+int se_get_profile(se_ctx* ctx, se_profile* prof);
+
+/* Waits for all work queued on the context's stream. */
+int se_synchronize(se_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SHAPEX_H */

@@ -1,0 +1,439 @@
+// Exact kNN over the search hierarchy, fused with covariance, 3x3 symmetric
+// eigensolve and orientation (sm_100a).
+//
+// Replaces, from the reference (paths relative to its project root):
+//   knnSearchKernel<k> + nodeBoxDistance + PriorityQueue
+//       src/Octree.hpp:136-212, src/Octree.cu:326-352, src/dequeue.hpp
+//   findCovariancesKernel<k>            src/NormalEstimation.hpp:96-156
+//   cusolverDnSsyevjBatched             src/NormalEstimation.hpp:235-301
+//   normalsFromEigenVectors             src/NormalEstimation.hpp:158-192
+//
+// One warp serves 32 consecutive queries (Morton-ordered, so spatially
+// coherent). Each lane keeps its query's k best (squared distance, index)
+// pairs sorted in registers. The warp first scans the Morton window around its
+// queries (seeding every lane's bound), then walks the search hierarchy depth
+// first with a shared stack: a child is entered when any lane's bound reaches
+// its box, nearer child first by lane vote; buckets (contiguous runs of at most
+// `bucket` points) are streamed through registers and broadcast by shuffles.
+// Pruning uses the box distance computed with the same rounding chain as the
+// point distance, so results are exact, ties broken by point index.
+
+#include <cfloat>
+#include <climits>
+#include <cstdint>
+
+#include "pipeline.cuh"
+
+namespace shapex {
+
+namespace {
+
+constexpr int kKnnThreads = 128;
+constexpr int kKnnWarps = kKnnThreads / 32;
+constexpr int kStackDepth = 96;
+constexpr int kSeedHalo = 16;
+constexpr unsigned FULL = 0xffffffffu;
+
+template <int K, bool EXACT>
+struct TopK {
+    float d[K];
+    int32_t id[K];
+    float bd;
+    int32_t bi;
+    int kk;
+    __device__ __forceinline__ void init(int k) {
+#pragma unroll
+        for (int j = 0; j < K; ++j) { d[j] = INFINITY; id[j] = INT_MAX; }
+        bd = INFINITY;
+        bi = INT_MAX;
+        kk = k;
+    }
+    __device__ __forceinline__ bool better(float dd, int32_t ii) const { return dd < bd || (dd == bd && ii < bi); }
+    __device__ __forceinline__ void insert(float dd, int32_t ii) {
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            const bool lt = dd < d[j] || (dd == d[j] && ii < id[j]);
+            const float td = d[j];
+            const int32_t ti = id[j];
+            d[j] = lt ? dd : td;
+            id[j] = lt ? ii : ti;
+            dd = lt ? td : dd;
+            ii = lt ? ti : ii;
+        }
+        if (EXACT) {
+            bd = d[K - 1];
+            bi = id[K - 1];
+        } else {
+#pragma unroll
+            for (int j = 0; j < K; ++j)
+                if (j == kk - 1) { bd = d[j]; bi = id[j]; }
+        }
+    }
+    __device__ __forceinline__ void consider(float dd, int32_t ii) {
+        if (better(dd, ii)) insert(dd, ii);
+    }
+};
+
+struct QArgs {
+    int k;
+    int64_t start, count, u;
+    const float* ext;
+    int32_t* out_idx;
+    float* out_d2;
+    float* out_normals;
+    float vx, vy, vz;
+    float gap;
+    int code_bits;
+    int bucket;
+};
+
+// ---- 3x3 symmetric eigensolver: cyclic Jacobi (Golub & Van Loan, Matrix
+// Computations, 4th ed., Alg. 8.5.2 sym.schur2 + 8.5.3), explicit indices ----
+template <typename T>
+__device__ __forceinline__ T rsqrt_t(T x);
+template <>
+__device__ __forceinline__ float rsqrt_t<float>(float x) { return 1.0f / sqrtf(x); }
+template <>
+__device__ __forceinline__ double rsqrt_t<double>(double x) { return 1.0 / sqrt(x); }
+
+template <int P, int Q, typename T>
+__device__ __forceinline__ void jrot(T (&A)[3][3], T (&V)[3][3]) {
+    const T apq = A[P][Q];
+    if (apq == T(0)) return;
+    constexpr int R = 3 - P - Q;
+    const T theta = (A[Q][Q] - A[P][P]) / (T(2) * apq);
+    const T at = fabs(theta);
+    T t;
+    if (at > T(1e15)) t = T(0.5) / theta;
+    else t = (theta >= T(0) ? T(1) : T(-1)) / (at + sqrt(theta * theta + T(1)));
+    const T c = rsqrt_t<T>(t * t + T(1));
+    const T s = t * c;
+    A[P][P] -= t * apq;
+    A[Q][Q] += t * apq;
+    A[P][Q] = A[Q][P] = T(0);
+    const T arp = A[R][P], arq = A[R][Q];
+    A[R][P] = A[P][R] = c * arp - s * arq;
+    A[R][Q] = A[Q][R] = s * arp + c * arq;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const T vkp = V[k][P], vkq = V[k][Q];
+        V[k][P] = c * vkp - s * vkq;
+        V[k][Q] = s * vkp + c * vkq;
+    }
+}
+
+// Returns the eigenvector of the smallest eigenvalue in n, and the ascending
+// eigenvalues in w.
+template <typename T>
+__device__ __forceinline__ void eig3(const T (&C)[6], T (&w)[3], T (&n)[3]) {
+    T A[3][3] = {{C[0], C[1], C[2]}, {C[1], C[3], C[4]}, {C[2], C[4], C[5]}};
+    T V[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    const T eps2 = sizeof(T) == 4 ? T(1e-14) : T(1e-30);
+    const int sweeps = sizeof(T) == 4 ? 12 : 20;
+    for (int s = 0; s < sweeps; ++s) {
+        const T off = A[0][1] * A[0][1] + A[0][2] * A[0][2] + A[1][2] * A[1][2];
+        const T dia = A[0][0] * A[0][0] + A[1][1] * A[1][1] + A[2][2] * A[2][2];
+        if (!(off > eps2 * dia)) break;
+        jrot<0, 1>(A, V);
+        jrot<0, 2>(A, V);
+        jrot<1, 2>(A, V);
+    }
+    const T e0 = A[0][0], e1 = A[1][1], e2 = A[2][2];
+    // ascending order with a stable tie rule (lower column first)
+    int i0 = 0, i1 = 1, i2 = 2;
+    T a0 = e0, a1 = e1, a2 = e2;
+    if (a1 < a0) { T t = a0; a0 = a1; a1 = t; int ti = i0; i0 = i1; i1 = ti; }
+    if (a2 < a1) { T t = a1; a1 = a2; a2 = t; int ti = i1; i1 = i2; i2 = ti; }
+    if (a1 < a0) { T t = a0; a0 = a1; a1 = t; int ti = i0; i0 = i1; i1 = ti; }
+    w[0] = a0; w[1] = a1; w[2] = a2;
+    n[0] = i0 == 0 ? V[0][0] : (i0 == 1 ? V[0][1] : V[0][2]);
+    n[1] = i0 == 0 ? V[1][0] : (i0 == 1 ? V[1][1] : V[1][2]);
+    n[2] = i0 == 0 ? V[2][0] : (i0 == 1 ? V[2][1] : V[2][2]);
+}
+
+__device__ __forceinline__ void neu_add(float& s, float& c, float x) {
+    const float t = s + x;
+    if (fabsf(s) >= fabsf(x)) c += (s - t) + x;
+    else c += (x - t) + s;
+    s = t;
+}
+
+template <int K, bool EXACT>
+__device__ __forceinline__ void scan_bucket(int32_t first, int cnt, bool need, float qx, float qy, float qz,
+                                            TopK<K, EXACT>& tk, const float4* __restrict__ pts, int64_t w0,
+                                            int64_t w1, int lane) {
+    const float4 p = lane < cnt ? __ldg(pts + first + lane) : make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int t = 0; t < cnt; ++t) {
+        const float px = __shfl_sync(FULL, p.x, t);
+        const float py = __shfl_sync(FULL, p.y, t);
+        const float pz = __shfl_sync(FULL, p.z, t);
+        const int32_t idx = first + t;
+        if (need && (idx < w0 || idx >= w1)) tk.consider(dist2(qx, qy, qz, px, py, pz), idx);
+    }
+}
+
+template <int K, bool EXACT, bool EXT, bool NORMALS>
+__global__ void __launch_bounds__(kKnnThreads) k_knn(const float4* __restrict__ pts, const SNode* __restrict__ snodes,
+                                                     const uint64_t* __restrict__ codes, QArgs a, DevState* st) {
+    __shared__ int32_t s_stack[kKnnWarps][kStackDepth];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t q0 = ((int64_t)blockIdx.x * kKnnWarps + warp) * 32;
+    if (q0 >= a.count) return;  // whole warp
+    const int64_t qo = q0 + lane;
+    const bool active = qo < a.count;
+    const int64_t u = a.u;
+    float qx, qy, qz;
+    int64_t center;
+    if (EXT) {
+        const int64_t src = active ? qo : q0;
+        qx = __ldg(a.ext + 3 * src);
+        qy = __ldg(a.ext + 3 * src + 1);
+        qz = __ldg(a.ext + 3 * src + 2);
+        // seed window centre: position of the warp's first query's code
+        const float lx = __shfl_sync(FULL, qx, 0), ly = __shfl_sync(FULL, qy, 0), lz = __shfl_sync(FULL, qz, 0);
+        const float mn = st->min_coord, range = st->range;
+        const float fbs = (float)bitscale_of(a.code_bits);
+        auto q1 = [&](float v) {
+            float f = __fmul_rn(fbs, __fdiv_rn(__fsub_rn(v, mn), range));
+            f = fminf(fmaxf(f, 0.0f), fbs);
+            return __float2uint_rz(f);
+        };
+        const uint64_t code = spread3(q1(lx)) | (spread3(q1(ly)) << 1) | (spread3(q1(lz)) << 2);
+        int64_t lo = 0, hi = u;
+        while (lo < hi) {
+            const int64_t mid = (lo + hi) >> 1;
+            if (__ldg(codes + mid) < code) lo = mid + 1; else hi = mid;
+        }
+        center = lo - 16;
+    } else {
+        const float4 p = __ldg(pts + a.start + (active ? qo : q0));
+        qx = p.x;
+        qy = p.y;
+        qz = p.z;
+        center = a.start + q0;
+    }
+    const int64_t w0 = max64(0, center - kSeedHalo);
+    const int64_t w1 = min64(u, center + 32 + kSeedHalo);
+
+    TopK<K, EXACT> tk;
+    tk.init(a.k);
+    for (int64_t b = w0; b < w1; b += 32) {
+        const int cnt = (int)min64(32, w1 - b);
+        const float4 p = lane < cnt ? __ldg(pts + b + lane) : make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int t = 0; t < cnt; ++t) {
+            const float px = __shfl_sync(FULL, p.x, t);
+            const float py = __shfl_sync(FULL, p.y, t);
+            const float pz = __shfl_sync(FULL, p.z, t);
+            if (active) tk.consider(dist2(qx, qy, qz, px, py, pz), (int32_t)(b + t));
+        }
+    }
+
+    uint32_t steps = 0;
+    if (u >= 2 && (w0 > 0 || w1 < u)) {
+        int sp = 1;
+        if (lane == 0) s_stack[warp][0] = 0;
+        __syncwarp();
+        const uint32_t cap = (uint32_t)min64(u + 64, 0x7fffffff);
+        while (sp > 0) {
+            --sp;
+            const int32_t node = s_stack[warp][sp];
+            __syncwarp();
+            if (++steps > cap || node < 0 || node >= u - 1) {
+                if (lane == 0) set_err(&st->err, steps > cap ? ERRBIT_SEARCH_LIMIT : ERRBIT_BOUNDS);
+                break;
+            }
+            const SNode* sn = snodes + node;
+            const float4 lo_l = __ldg(&sn->lo_l), hi_l = __ldg(&sn->hi_l);
+            const float4 lo_r = __ldg(&sn->lo_r), hi_r = __ldg(&sn->hi_r);
+            const int32_t ref[2] = {__float_as_int(lo_l.w), __float_as_int(lo_r.w)};
+            const int32_t cnt[2] = {__float_as_int(hi_l.w), __float_as_int(hi_r.w)};
+            if (cnt[0] < 1 || cnt[1] < 1 || ref[0] < 0 || ref[1] < 0 ||
+                (cnt[0] <= a.bucket ? (int64_t)ref[0] + cnt[0] > u : ref[0] >= u - 1) ||
+                (cnt[1] <= a.bucket ? (int64_t)ref[1] + cnt[1] > u : ref[1] >= u - 1)) {
+                if (lane == 0) set_err(&st->err, ERRBIT_BOUNDS);
+                break;
+            }
+            const float dl = box_dist2(qx, qy, qz, lo_l.x, lo_l.y, lo_l.z, hi_l.x, hi_l.y, hi_l.z);
+            const float dr = box_dist2(qx, qy, qz, lo_r.x, lo_r.y, lo_r.z, hi_r.x, hi_r.y, hi_r.z);
+            const uint32_t bl = __ballot_sync(FULL, active && dl <= tk.bd);
+            const uint32_t br = __ballot_sync(FULL, active && dr <= tk.bd);
+            if (!(bl | br)) continue;
+            const uint32_t vote = __ballot_sync(FULL, active && dl <= dr);
+            const int nact = __popc(__ballot_sync(FULL, active));
+            const int firstSide = (2 * __popc(vote) >= nact) ? 0 : 1;
+#pragma unroll
+            for (int o = 0; o < 2; ++o) {
+                const int side = o ? 1 - firstSide : firstSide;
+                if (cnt[side] > a.bucket) continue;
+                const float ds = side ? dr : dl;
+                const bool need = active && ds <= tk.bd;
+                if (!__ballot_sync(FULL, need)) continue;
+                scan_bucket<K, EXACT>(ref[side], cnt[side], need, qx, qy, qz, tk, pts, w0, w1, lane);
+            }
+#pragma unroll
+            for (int o = 1; o >= 0; --o) {
+                const int side = o ? 1 - firstSide : firstSide;
+                if (cnt[side] <= a.bucket || !(side ? br : bl)) continue;
+                if (sp >= kStackDepth) {
+                    if (lane == 0) set_err(&st->err, ERRBIT_STACK);
+                    continue;
+                }
+                if (lane == 0) s_stack[warp][sp] = ref[side];
+                ++sp;
+            }
+            __syncwarp();
+        }
+    }
+    if (lane == 0 && steps) atomicAdd(&st->nodes_visited, (unsigned long long)steps);
+    if (!active) return;
+
+    // fewer than k points in the tree: repeat entry 0 (src/Octree.hpp:181-191)
+#pragma unroll
+    for (int j = 1; j < K; ++j)
+        if (j < a.k && tk.id[j] == INT_MAX) { tk.id[j] = tk.id[0]; tk.d[j] = tk.d[0]; }
+
+    if (a.out_idx) {
+        int32_t* o = a.out_idx + qo * a.k;
+#pragma unroll
+        for (int j = 0; j < K; ++j)
+            if (j < a.k) o[j] = tk.id[j];
+    }
+    if (a.out_d2) {
+        float* o = a.out_d2 + qo * a.k;
+#pragma unroll
+        for (int j = 0; j < K; ++j)
+            if (j < a.k) o[j] = tk.d[j];
+    }
+    if (NORMALS) {
+        const int k = a.k;
+        // centroid of the neighbours relative to the query, compensated sums
+        float s[3] = {0.f, 0.f, 0.f}, c[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            if (j < k) {
+                const float4 p = __ldg(pts + tk.id[j]);
+                neu_add(s[0], c[0], p.x - qx);
+                neu_add(s[1], c[1], p.y - qy);
+                neu_add(s[2], c[2], p.z - qz);
+            }
+        }
+        const float inv_k = 1.0f / (float)k;
+        const float m0 = (s[0] + c[0]) * inv_k, m1 = (s[1] + c[1]) * inv_k, m2 = (s[2] + c[2]) * inv_k;
+        float cs[6] = {0, 0, 0, 0, 0, 0}, cc[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            if (j < k) {
+                const float4 p = __ldg(pts + tk.id[j]);
+                const float r0 = (p.x - qx) - m0, r1 = (p.y - qy) - m1, r2 = (p.z - qz) - m2;
+                neu_add(cs[0], cc[0], r0 * r0);
+                neu_add(cs[1], cc[1], r0 * r1);
+                neu_add(cs[2], cc[2], r0 * r2);
+                neu_add(cs[3], cc[3], r1 * r1);
+                neu_add(cs[4], cc[4], r1 * r2);
+                neu_add(cs[5], cc[5], r2 * r2);
+            }
+        }
+        const float inv_den = 1.0f / (float)(k > 1 ? k - 1 : 1);
+        float C[6];
+#pragma unroll
+        for (int e = 0; e < 6; ++e) C[e] = (cs[e] + cc[e]) * inv_den;
+        float w[3], nv[3];
+        eig3<float>(C, w, nv);
+        float nx = nv[0], ny = nv[1], nz = nv[2];
+        const float gap = (w[1] - w[0]) / fmaxf(fabsf(w[2]), FLT_MIN);
+        if (!(gap >= a.gap)) {
+            // near-degenerate neighbourhood: redo covariance and eigensolve in FP64
+            double sd[3] = {0, 0, 0};
+#pragma unroll
+            for (int j = 0; j < K; ++j) {
+                if (j < k) {
+                    const float4 p = __ldg(pts + tk.id[j]);
+                    sd[0] += (double)p.x - (double)qx;
+                    sd[1] += (double)p.y - (double)qy;
+                    sd[2] += (double)p.z - (double)qz;
+                }
+            }
+            const double md[3] = {sd[0] / k, sd[1] / k, sd[2] / k};
+            double Cd[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+            for (int j = 0; j < K; ++j) {
+                if (j < k) {
+                    const float4 p = __ldg(pts + tk.id[j]);
+                    const double r0 = ((double)p.x - (double)qx) - md[0];
+                    const double r1 = ((double)p.y - (double)qy) - md[1];
+                    const double r2 = ((double)p.z - (double)qz) - md[2];
+                    Cd[0] += r0 * r0; Cd[1] += r0 * r1; Cd[2] += r0 * r2;
+                    Cd[3] += r1 * r1; Cd[4] += r1 * r2; Cd[5] += r2 * r2;
+                }
+            }
+            const double dd = (double)(k > 1 ? k - 1 : 1);
+#pragma unroll
+            for (int e = 0; e < 6; ++e) Cd[e] /= dd;
+            double wd[3], nd[3];
+            eig3<double>(Cd, wd, nd);
+            nx = (float)nd[0];
+            ny = (float)nd[1];
+            nz = (float)nd[2];
+            atomicAdd(&st->fp64_solves, 1ull);
+        }
+        // orientation towards the viewpoint (src/NormalEstimation.hpp:184-189)
+        const float dot = (a.vx - qx) * nx + (a.vy - qy) * ny + (a.vz - qz) * nz;
+        if (dot < 0.0f) { nx = -nx; ny = -ny; nz = -nz; }
+        float* o = a.out_normals + 3 * qo;
+        o[0] = nx;
+        o[1] = ny;
+        o[2] = nz;
+    }
+}
+
+template <int K, bool EXACT>
+cudaError_t launch_k(const BuildBufs& b, const QArgs& a, bool ext, bool normals, cudaStream_t s) {
+    const int64_t warps = (a.count + 31) / 32;
+    const unsigned blocks = (unsigned)((warps + kKnnWarps - 1) / kKnnWarps);
+    if (ext)
+        k_knn<K, EXACT, true, false><<<blocks, kKnnThreads, 0, s>>>(b.pts4, b.snodes, b.codes, a, b.st);
+    else if (normals)
+        k_knn<K, EXACT, false, true><<<blocks, kKnnThreads, 0, s>>>(b.pts4, b.snodes, b.codes, a, b.st);
+    else
+        k_knn<K, EXACT, false, false><<<blocks, kKnnThreads, 0, s>>>(b.pts4, b.snodes, b.codes, a, b.st);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t enqueue_query(const BuildBufs& b, const QueryParams& q, cudaStream_t s, int /*num_sms*/) {
+    if (q.count <= 0) return cudaSuccess;
+    QArgs a;
+    a.k = q.k;
+    a.start = q.start;
+    a.count = q.count;
+    a.u = q.u;
+    a.ext = q.ext_queries;
+    a.out_idx = q.out_idx;
+    a.out_d2 = q.out_d2;
+    a.out_normals = q.out_normals;
+    a.vx = q.vx;
+    a.vy = q.vy;
+    a.vz = q.vz;
+    a.gap = q.eigengap_fp64;
+    a.code_bits = q.code_bits;
+    a.bucket = q.bucket;
+    const bool ext = q.ext_queries != nullptr;
+    const bool nrm = q.out_normals != nullptr && !ext;
+    switch (q.k) {
+        case 8: return launch_k<8, true>(b, a, ext, nrm, s);
+        case 10: return launch_k<10, true>(b, a, ext, nrm, s);
+        case 16: return launch_k<16, true>(b, a, ext, nrm, s);
+        case 32: return launch_k<32, true>(b, a, ext, nrm, s);
+        default: break;
+    }
+    if (q.k < 1 || q.k > 32) return cudaErrorInvalidValue;
+    if (q.k <= 4) return launch_k<4, false>(b, a, ext, nrm, s);
+    if (q.k <= 8) return launch_k<8, false>(b, a, ext, nrm, s);
+    if (q.k <= 12) return launch_k<12, false>(b, a, ext, nrm, s);
+    if (q.k <= 16) return launch_k<16, false>(b, a, ext, nrm, s);
+    if (q.k <= 24) return launch_k<24, false>(b, a, ext, nrm, s);
+    return launch_k<32, false>(b, a, ext, nrm, s);
+}
+
+}  // namespace shapex

@@ -1,0 +1,136 @@
+// Internal interface between the C ABI layer (capi.cu) and the kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace shapex {
+
+constexpr int kSortPasses = 8;
+constexpr int kSortThreads = 512;
+constexpr int kSortIpt = 8;
+constexpr int kSortTile = kSortThreads * kSortIpt;  // 4096 keys per tile
+constexpr int kDedupThreads = 256;
+constexpr int kDedupIpt = 16;
+constexpr int kDedupTile = kDedupThreads * kDedupIpt;
+constexpr int kScanThreads = 256;
+constexpr int kScanIpt = 16;
+constexpr int kScanTile = kScanThreads * kScanIpt;
+
+// Small device-resident state of one build (zeroed at the start of each build).
+struct DevState {
+    uint32_t err;
+    uint32_t min_ord;  // ordered-uint encodings (f2ord) of the bbox min / max
+    uint32_t max_ord;
+    uint32_t pad0;
+    float min_coord, max_coord, range;
+    int32_t n_active;                       // non-trivial sort passes
+    int32_t pass_active[kSortPasses];
+    int32_t pass_parity[kSortPasses];
+    uint32_t tile_counter[16];              // dynamic tile ids: sort passes, dedup, octree scan
+    uint32_t hist[kSortPasses][256];        // per-digit histograms of the codes
+    uint32_t digit_off[kSortPasses][256];   // exclusive digit offsets
+    unsigned long long u;                   // unique codes
+    unsigned long long n_oct;               // octree nodes
+    int32_t root_level;
+    // fixed-root description used by the search hierarchy (node 0)
+    int32_t sroot_gamma;
+    int32_t sroot_hl, sroot_hr;
+    unsigned long long fp64_solves;
+    unsigned long long nodes_visited;
+};
+
+// Byte layout of OT::OTNode (reference src/Octree.hpp:19-36), 56 bytes.
+struct OtNode {
+    int32_t children[8];
+    float corner[3];
+    float cell_size;
+    int32_t child_node_mask;
+    int32_t child_leaf_mask;
+};
+static_assert(sizeof(OtNode) == 56, "OTNode layout");
+
+// Search hierarchy node: internal node of the binary radix tree (root range
+// always [0, u-1]) holding both children's tight point boxes. A child with at
+// most `bucket` points is a bucket: ref = first point index, points
+// [ref, ref + cnt) are contiguous in Morton order. Otherwise ref = node index.
+struct __align__(16) SNode {
+    float4 lo_l;  // .w: ref of the left child (int bits)
+    float4 hi_l;  // .w: point count of the left child (int bits)
+    float4 lo_r;
+    float4 hi_r;
+};
+
+struct BuildBufs {
+    int64_t cap;  // capacity in points
+    const float* x;
+    const float* y;
+    const float* z;
+    uint64_t* keys0;
+    uint64_t* keys1;
+    uint32_t* lookback;  // sort/dedup look-back words
+    unsigned long long* lookback64;  // octree-scan look-back words
+    uint64_t* codes;     // unique sorted codes
+    float4* pts4;        // decoded points, padded for 16-byte loads
+    float* pts3;         // decoded points, AoS xyz
+    // radix tree as exported (RT::Nodes)
+    int32_t* left_child;
+    int32_t* parent;
+    uint8_t* prefix_n;
+    uint8_t* has_leaf_left;
+    uint8_t* has_leaf_right;
+    // search hierarchy
+    int32_t* sparent;
+    int32_t* leaf_parent;
+    int32_t* range_end;
+    uint32_t* visit;
+    float4* node_box;  // 2 per node: lo, hi
+    SNode* snodes;
+    // octree
+    int32_t* oct_counts;
+    int32_t* oct_offsets;  // cap + 1
+    void* oct_nodes;       // se_otnode[oct_cap]
+    int64_t oct_cap;
+    DevState* st;
+};
+
+struct BuildParams {
+    int64_t n;
+    int code_bits;
+    int root_compat;
+    int build_octree;
+    int bucket;
+};
+
+// Stage events of one build: [0] start, then after bbox, encode, sort, dedup,
+// radix tree, search boxes, octree.
+constexpr int kBuildEvents = 8;
+
+// Enqueue the whole build on `s`. Reads x/y/z from bufs; results stay on the
+// device. `ev` (kBuildEvents events, may be null) are recorded between stages;
+// *launches receives the number of kernels launched.
+cudaError_t enqueue_build(const BuildBufs& b, const BuildParams& p, cudaStream_t s, int num_sms, cudaEvent_t* ev,
+                          int* launches);
+// Enqueue only the octree stage (used to redo it after a capacity regrow).
+cudaError_t enqueue_octree(const BuildBufs& b, const BuildParams& p, cudaStream_t s, int num_sms, int* launches);
+
+struct QueryParams {
+    int k;
+    int64_t start;      // first query (self queries)
+    int64_t count;      // number of queries
+    int64_t u;          // tree points
+    const float* ext_queries;  // AoS xyz external queries or nullptr (self queries)
+    int32_t* out_idx;   // count*k or nullptr
+    float* out_d2;      // count*k or nullptr
+    float* out_normals; // count*3 or nullptr
+    float vx, vy, vz;
+    float eigengap_fp64;
+    int code_bits;
+    int bucket;
+};
+
+cudaError_t enqueue_query(const BuildBufs& b, const QueryParams& q, cudaStream_t s, int num_sms);
+
+}  // namespace shapex

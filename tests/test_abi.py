@@ -1,0 +1,62 @@
+"""CPU checks of the C ABI library: it builds for sm_100a, loads, exports every
+entry point include/shapex.h declares, and fails with a status (not a crash)
+when no sm_100 device is present. No compute call is made here."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from conftest import ROOT
+
+
+def header_functions():
+    src = open(os.path.join(ROOT, "include", "shapex.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(se_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_header_lists_entry_points():
+    names = header_functions()
+    for must in ("se_create", "se_build", "se_normals", "se_knn", "se_knn_self", "se_get_octree"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol(native):
+    L = native.lib()
+    declared = header_functions()
+    for name in declared:
+        assert hasattr(L, name), name
+    assert sorted(native.EXPORTS) == declared
+
+
+def test_library_is_sm100a_only(native):
+    # the fatbin carries sm_100a code: its ELF notes name the arch
+    blob = open(native.LIB_PATH, "rb").read()
+    assert b"sm_100a" in blob
+
+
+def test_options_defaults(native):
+    L = native.lib()
+    o = native.SeOptions()
+    assert L.se_options_init(ctypes.byref(o)) == 0
+    assert o.code_bits == 63 and o.root_compat == 1 and o.build_octree == 1
+    assert tuple(o.viewpoint) == (0.0, 0.0, 0.0)
+    assert L.se_abi_version() == 1
+    assert L.se_status_string(5) == b"SE_ERR_NONFINITE"
+
+
+def test_null_context_is_rejected(native):
+    L = native.lib()
+    assert L.se_build(None, None, None, None, 0, 0) == 1
+    assert L.se_normals(None, 16, 0, 1, None, 0) == 1
+    assert L.se_options_init(None) == 1
+
+
+def test_create_without_gpu_fails_cleanly(native):
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(native.ShapexError):
+        native.Context()
