@@ -145,7 +145,7 @@ def octree_check(nodes, codes, code_bits, root_level):
     return rc, seen
 
 
-def knn_compat(nodes, pts, queries, k, dist_variant=0, want_pops=False):
+def knn_compat(nodes, pts, queries, k, dist_variant=1, want_pops=False):
     pts = _f32(pts)
     queries = _f32(queries)
     nq = queries.shape[0]
