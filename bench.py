@@ -93,7 +93,7 @@ class Clocks:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
@@ -151,7 +151,7 @@ def run_ours(a):
     dx, dy, dz = (v.cuda() for v in (hx, hy, hz))
     stream = torch.cuda.current_stream()
     ctx = Context(code_bits=wl["code_bits"], device=local, stream=stream.cuda_stream,
-                  eigengap_fp64=a.eigengap, leaf_bucket=a.bucket)
+                  eigengap_fp64=a.eigengap, leaf_bucket=a.bucket, seed_halo=a.halo)
     u = ctx.build(dx, dy, dz)["n_points"]
     out_dev = torch.empty((u, 3), dtype=torch.float32, device="cuda")
     out_host = torch.empty((u, 3), dtype=torch.float32).pin_memory()
@@ -235,7 +235,7 @@ def run_ours(a):
                        "k": k, "code_bits": wl["code_bits"], "octree_nodes": int(m),
                        "l2": "flushed by a 256 MB device write before every timed step",
                        "parallelism": f"{world} independent replica(s), one cloud per GPU",
-                       "leaf_bucket": a.bucket, "eigengap_fp64": a.eigengap},
+                       "leaf_bucket": a.bucket, "seed_halo": a.halo, "eigengap_fp64": a.eigengap},
             "e2e": {"value": u_all * a.steps / (ms_e2e * 1e-3), "unit": "normals/s",
                     "ms_per_step": ms_e2e / a.steps, "h2d_bytes_per_step": int(12 * n),
                     "d2h_bytes_per_step": int(12 * u)},
@@ -246,7 +246,9 @@ def run_ours(a):
             "stages_ms": {**build_ms, "knn_normals": q_ms},
             "gpu_launches": int(launches),
             "fp64_solves_last_step": stats["fp64_solves"],
-            "nodes_visited_per_query": stats["nodes_visited"] / max(u, 1) * 32,
+            "search_per_warp": {key: stats[key] / max(u / 32, 1) for key in
+                                ("nodes_visited", "buckets_scanned", "merge_steps")},
+            "search_per_query": {key: stats[key] / max(u, 1) for key in ("candidates", "inserts")},
             "clocks": clocks,
             "cpu_baseline": cpu,
         }
@@ -367,7 +369,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="scene_2M_k16")
     ap.add_argument("--seed", type=int, default=1)
-    ap.add_argument("--bucket", type=int, default=16)
+    ap.add_argument("--bucket", type=int, default=32)
+    ap.add_argument("--halo", type=int, default=16)
     ap.add_argument("--eigengap", type=float, default=1e-4)
     ap.add_argument("--cpu-sample", type=int, default=200_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")

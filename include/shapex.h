@@ -53,7 +53,9 @@ typedef struct se_options {
                               scanned directly (1..32; 0 = default) */
     int32_t device;        /* CUDA device ordinal */
     void* stream;          /* cudaStream_t to use; NULL: the context creates one */
-    int32_t reserved[8];
+    int32_t seed_halo;     /* kNN: points offered on each side of a warp's 32 queries
+                              before the tree walk (0..48; -1 = default) */
+    int32_t reserved[7];
 } se_options;
 
 /* Sizes after se_build (RT::RadixTree / OT::Octree public fields). */
@@ -146,9 +148,16 @@ int se_knn(se_ctx* ctx, int k, const float* queries_xyz, int64_t n_queries, int3
  * kernel. out_xyz: count normals, AoS xyz (std::vector<Point> layout). */
 int se_normals(se_ctx* ctx, int k, int64_t start, int64_t count, float* out_xyz, int mem);
 
-/* Counters of the last se_normals/se_knn call: queries whose eigensolve took
- * the FP64 path, and total tree nodes visited (diagnostics). */
-int se_get_stats(const se_ctx* ctx, int64_t* fp64_solves, int64_t* nodes_visited);
+/* Work counters of the last se_normals/se_knn/se_knn_self call (diagnostics). */
+typedef struct se_stats {
+    int64_t fp64_solves;     /* queries whose eigensolve took the FP64 path */
+    int64_t nodes_visited;   /* search-hierarchy nodes visited, summed over warps */
+    int64_t buckets_scanned; /* point buckets streamed, summed over warps */
+    int64_t candidates;      /* points that reached a query's bound, summed over queries */
+    int64_t merge_steps;     /* candidate-buffer merge steps, summed over warps */
+    int64_t inserts;         /* insertions into the k-best lists, summed over queries */
+} se_stats;
+int se_get_stats(const se_ctx* ctx, se_stats* stats);
 
 /* Device timings of the last se_build and query call, from CUDA events
  * recorded on the context's stream around each stage, and the number of

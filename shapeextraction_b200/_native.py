@@ -41,7 +41,8 @@ class SeOptions(ctypes.Structure):
     _fields_ = [
         ("code_bits", ctypes.c_int32), ("root_compat", ctypes.c_int32), ("build_octree", ctypes.c_int32),
         ("viewpoint", ctypes.c_float * 3), ("eigengap_fp64", ctypes.c_float), ("leaf_bucket", ctypes.c_int32),
-        ("device", ctypes.c_int32), ("stream", ctypes.c_void_p), ("reserved", ctypes.c_int32 * 8),
+        ("device", ctypes.c_int32), ("stream", ctypes.c_void_p), ("seed_halo", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 7),
     ]
 
 
@@ -56,6 +57,13 @@ class SeInfo(ctypes.Structure):
 class SeDeviceViews(ctypes.Structure):
     _fields_ = [(n, ctypes.c_void_p) for n in (
         "codes", "points", "octree", "left_child", "parent", "prefix_n", "has_leaf_left", "has_leaf_right")]
+
+
+STAT_NAMES = ["fp64_solves", "nodes_visited", "buckets_scanned", "candidates", "merge_steps", "inserts"]
+
+
+class SeStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in STAT_NAMES]
 
 
 class SeProfile(ctypes.Structure):
@@ -101,7 +109,7 @@ def lib():
             "se_knn_self": (i32, [P, i32, i64, i64, P, P, i32]),
             "se_knn": (i32, [P, i32, P, i64, P, P, i32]),
             "se_normals": (i32, [P, i32, i64, i64, P, i32]),
-            "se_get_stats": (i32, [P, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]),
+            "se_get_stats": (i32, [P, ctypes.POINTER(SeStats)]),
             "se_get_profile": (i32, [P, ctypes.POINTER(SeProfile)]),
             "se_synchronize": (i32, [P]),
         }
@@ -134,7 +142,7 @@ class Context:
     """One se_ctx: device memory and a CUDA stream for one host thread."""
 
     def __init__(self, code_bits=63, root_compat=True, build_octree=True, viewpoint=(0.0, 0.0, 0.0),
-                 eigengap_fp64=1e-4, leaf_bucket=16, device=0, stream=None):
+                 eigengap_fp64=1e-4, leaf_bucket=32, device=0, stream=None, seed_halo=16):
         L = lib()
         o = SeOptions()
         L.se_options_init(ctypes.byref(o))
@@ -147,6 +155,7 @@ class Context:
         o.leaf_bucket = int(leaf_bucket)
         o.device = int(device)
         o.stream = stream
+        o.seed_halo = int(seed_halo)
         self.options = o
         h = ctypes.c_void_p()
         rc = L.se_create(ctypes.byref(h), ctypes.byref(o))
@@ -278,9 +287,9 @@ class Context:
         return o
 
     def stats(self):
-        a, b = ctypes.c_int64(), ctypes.c_int64()
-        lib().se_get_stats(self._h, ctypes.byref(a), ctypes.byref(b))
-        return {"fp64_solves": a.value, "nodes_visited": b.value}
+        st = SeStats()
+        self._check(lib().se_get_stats(self._h, ctypes.byref(st)), "se_get_stats")
+        return {n: getattr(st, n) for n in STAT_NAMES}
 
     def profile(self):
         p = SeProfile()

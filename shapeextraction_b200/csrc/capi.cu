@@ -33,7 +33,7 @@ struct se_ctx {
 
     bool built = false;
     se_info info{};
-    int64_t last_fp64 = 0, last_visited = 0;
+    int64_t last_counters[kQueryCounters] = {};
 
     cudaEvent_t build_ev[kBuildEvents] = {};
     cudaEvent_t query_ev[2] = {};
@@ -182,6 +182,7 @@ int run_query(se_ctx* c, int k, int64_t start, int64_t count, const float* ext, 
     q.eigengap_fp64 = c->opt.eigengap_fp64;
     q.code_bits = c->opt.code_bits;
     q.bucket = c->opt.leaf_bucket;
+    q.seed_halo = c->opt.seed_halo;
     const bool host = mem == SE_MEM_HOST;
     if (ext) {
         if (host) {
@@ -223,7 +224,7 @@ int run_query(se_ctx* c, int k, int64_t start, int64_t count, const float* ext, 
     }
     // clear the error word and counters of the previous call
     SE_CUDA(c, cudaMemsetAsync(&c->b.st->err, 0, sizeof(uint32_t), c->stream), "reset");
-    SE_CUDA(c, cudaMemsetAsync(&c->b.st->fp64_solves, 0, 2 * sizeof(unsigned long long), c->stream), "reset");
+    SE_CUDA(c, cudaMemsetAsync(c->b.st->counters, 0, sizeof(c->b.st->counters), c->stream), "reset");
     c->have_query_times = false;
     SE_CUDA(c, cudaEventRecord(c->query_ev[0], c->stream), "event");
     SE_CUDA(c, enqueue_query(c->b, q, c->stream, c->num_sms), "launch query");
@@ -244,12 +245,11 @@ int run_query(se_ctx* c, int k, int64_t start, int64_t count, const float* ext, 
     }
     SE_CUDA(c, cudaMemcpyAsync(&c->h_st->err, &c->b.st->err, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream),
             "read state");
-    SE_CUDA(c, cudaMemcpyAsync(&c->h_st->fp64_solves, &c->b.st->fp64_solves, 2 * sizeof(unsigned long long),
+    SE_CUDA(c, cudaMemcpyAsync(c->h_st->counters, c->b.st->counters, sizeof(c->b.st->counters),
                                cudaMemcpyDeviceToHost, c->stream),
             "read state");
     SE_CUDA(c, cudaStreamSynchronize(c->stream), "synchronize");
-    c->last_fp64 = (int64_t)c->h_st->fp64_solves;
-    c->last_visited = (int64_t)c->h_st->nodes_visited;
+    for (int i = 0; i < kQueryCounters; ++i) c->last_counters[i] = (int64_t)c->h_st->counters[i];
     return check_err_bits(c, c->h_st->err);
 }
 
@@ -267,9 +267,10 @@ int se_options_init(se_options* o) {
     o->build_octree = 1;
     o->viewpoint[0] = o->viewpoint[1] = o->viewpoint[2] = 0.0f;
     o->eigengap_fp64 = 1e-4f;
-    o->leaf_bucket = 16;
+    o->leaf_bucket = 32;
     o->device = 0;
     o->stream = nullptr;
+    o->seed_halo = 16;
     return SE_OK;
 }
 
@@ -295,8 +296,10 @@ int se_create(se_ctx** out, const se_options* opt) {
     se_options o;
     if (opt) o = *opt; else se_options_init(&o);
     if (o.code_bits != 63 && o.code_bits != 30) return SE_ERR_INVALID_ARG;
-    if (o.leaf_bucket == 0) o.leaf_bucket = 16;
+    if (o.leaf_bucket == 0) o.leaf_bucket = 32;
     if (o.leaf_bucket < 1 || o.leaf_bucket > 32) return SE_ERR_INVALID_ARG;
+    if (o.seed_halo < 0) o.seed_halo = 16;
+    if (o.seed_halo > 48) return SE_ERR_INVALID_ARG;
     if (!(o.eigengap_fp64 >= 0.0f)) return SE_ERR_INVALID_ARG;
     se_ctx* c = new se_ctx();
     c->opt = o;
@@ -500,10 +503,10 @@ int se_normals(se_ctx* c, int k, int64_t start, int64_t count, float* out, int m
     return run_query(c, k, start, count, nullptr, nullptr, nullptr, out, mem);
 }
 
-int se_get_stats(const se_ctx* c, int64_t* fp64_solves, int64_t* nodes_visited) {
-    if (!c) return SE_ERR_INVALID_ARG;
-    if (fp64_solves) *fp64_solves = c->last_fp64;
-    if (nodes_visited) *nodes_visited = c->last_visited;
+int se_get_stats(const se_ctx* c, se_stats* out) {
+    if (!c || !out) return SE_ERR_INVALID_ARG;
+    static_assert(sizeof(se_stats) == sizeof(int64_t) * kQueryCounters, "se_stats layout");
+    std::memcpy(out, c->last_counters, sizeof(*out));
     return SE_OK;
 }
 

@@ -9,14 +9,18 @@
 //   normalsFromEigenVectors             src/NormalEstimation.hpp:158-192
 //
 // One warp serves 32 consecutive queries (Morton-ordered, so spatially
-// coherent). Each lane keeps its query's k best (squared distance, index)
-// pairs sorted in registers. The warp first scans the Morton window around its
-// queries (seeding every lane's bound), then walks the search hierarchy depth
-// first with a shared stack: a child is entered when any lane's bound reaches
-// its box, nearer child first by lane vote; buckets (contiguous runs of at most
-// `bucket` points) are streamed through registers and broadcast by shuffles.
-// Pruning uses the box distance computed with the same rounding chain as the
-// point distance, so results are exact, ties broken by point index.
+// coherent); lane i owns query i. Each lane keeps its k best (squared
+// distance, index) keys in a max-heap in shared memory, whose root is the
+// lane's pruning bound. The warp first offers the Morton window around its
+// queries, then walks the search hierarchy depth first with a shared stack: a
+// child is entered when any lane's bound reaches its box, nearer child first
+// by lane vote. Bucket points (contiguous runs of at most `bucket` points) are
+// staged in shared memory and read by broadcast. A point that reaches a lane's
+// bound goes to that lane's candidate buffer; buffers are merged into the
+// heaps in batches, so that the warp pays for one heap update per buffered
+// slot rather than one per point any lane accepts. Pruning uses the box
+// distance with the same rounding chain as the point distance, so the result
+// is exact, ties broken by point index.
 
 #include <cfloat>
 #include <climits>
@@ -31,47 +35,59 @@ namespace {
 constexpr int kKnnThreads = 128;
 constexpr int kKnnWarps = kKnnThreads / 32;
 constexpr int kStackDepth = 96;
-constexpr int kSeedHalo = 16;
+constexpr int kBuf = 32;                // per-lane candidate buffer slots
+constexpr int kMaxHalo = 48;            // seed points on each side of a warp's queries
+constexpr int kWindowMax = 32 + 2 * kMaxHalo;
 constexpr unsigned FULL = 0xffffffffu;
 
+// (squared distance, index) packed so that one unsigned compare orders by
+// distance then index; distances are >= 0, so their IEEE bits are monotonic.
+__device__ __forceinline__ unsigned long long pack_key(float d, int64_t i) {
+    return ((unsigned long long)__float_as_uint(d) << 32) | (uint32_t)i;
+}
+constexpr unsigned long long kEmptyKey = (0x7f800000ull << 32) | 0xffffffffull;  // (+inf, max index)
+__device__ __forceinline__ int32_t key_idx(unsigned long long k) { return (int32_t)(uint32_t)k; }
+__device__ __forceinline__ float key_d(unsigned long long k) { return __uint_as_float((uint32_t)(k >> 32)); }
+
+// The k best keys of one query, ascending, in registers. Insertion compares
+// the new key with every entry independently and shifts in one step (no
+// serial chain). With EXACT = false the list is longer than k and the bound
+// is entry k-1.
 template <int K, bool EXACT>
 struct TopK {
-    float d[K];
-    int32_t id[K];
-    float bd;
-    int32_t bi;
+    unsigned long long key[K];
+    unsigned long long bk;  // entry k-1: the pruning bound
     int kk;
     __device__ __forceinline__ void init(int k) {
 #pragma unroll
-        for (int j = 0; j < K; ++j) { d[j] = INFINITY; id[j] = INT_MAX; }
-        bd = INFINITY;
-        bi = INT_MAX;
+        for (int j = 0; j < K; ++j) key[j] = kEmptyKey;
+        bk = kEmptyKey;
         kk = k;
     }
-    __device__ __forceinline__ bool better(float dd, int32_t ii) const { return dd < bd || (dd == bd && ii < bi); }
-    __device__ __forceinline__ void insert(float dd, int32_t ii) {
+    __device__ __forceinline__ float tau() const { return key_d(bk); }
+    __device__ __forceinline__ void insert(unsigned long long nk) {  // requires nk < bk
+        bool lt[K];
 #pragma unroll
-        for (int j = 0; j < K; ++j) {
-            const bool lt = dd < d[j] || (dd == d[j] && ii < id[j]);
-            const float td = d[j];
-            const int32_t ti = id[j];
-            d[j] = lt ? dd : td;
-            id[j] = lt ? ii : ti;
-            dd = lt ? td : dd;
-            ii = lt ? ti : ii;
-        }
+        for (int j = 0; j < K; ++j) lt[j] = key[j] < nk;
+#pragma unroll
+        for (int j = K - 1; j >= 1; --j) key[j] = lt[j] ? key[j] : (lt[j - 1] ? nk : key[j - 1]);
+        key[0] = lt[0] ? key[0] : nk;
         if (EXACT) {
-            bd = d[K - 1];
-            bi = id[K - 1];
+            bk = key[K - 1];
         } else {
 #pragma unroll
             for (int j = 0; j < K; ++j)
-                if (j == kk - 1) { bd = d[j]; bi = id[j]; }
+                if (j == kk - 1) bk = key[j];
         }
     }
-    __device__ __forceinline__ void consider(float dd, int32_t ii) {
-        if (better(dd, ii)) insert(dd, ii);
-    }
+};
+
+// Per-warp shared scratch: traversal stack, staged points, candidate buffers
+// ([slot][lane] so that a warp's accesses to one slot fall in distinct banks).
+struct WarpSmem {
+    int32_t stack[kStackDepth];
+    float4 pts[kWindowMax];
+    unsigned long long buf[kBuf][32];
 };
 
 struct QArgs {
@@ -85,7 +101,54 @@ struct QArgs {
     float gap;
     int code_bits;
     int bucket;
+    int seed_halo;
 };
+
+struct Counters {
+    int cand = 0, ins = 0, merge = 0, buckets = 0;
+};
+
+// Merge every lane's buffered candidates into its list; the warp steps
+// through max-over-lanes slots together.
+template <int K, bool EXACT>
+__device__ __forceinline__ void flush(TopK<K, EXACT>& tk, int& bc, WarpSmem& W, int lane, Counters& ct) {
+    const int maxc = (int)__reduce_max_sync(FULL, (unsigned)bc);
+    ct.merge += maxc;
+    ct.cand += bc;
+    for (int j = 0; j < maxc; ++j) {
+        if (j < bc) {
+            const unsigned long long nk = W.buf[j][lane];
+            if (nk < tk.bk) {
+                tk.insert(nk);
+                ++ct.ins;
+            }
+        }
+    }
+    bc = 0;
+}
+
+// Stage points [first, first + cnt) (cnt <= 32) in shared memory and append
+// every one whose distance reaches the lane's bound to the lane's buffer.
+// Points of the seed window [w0, w1) are skipped (they were already offered).
+// The caller guarantees bc + cnt <= kBuf.
+__device__ __forceinline__ void scan_chunk(int32_t first, int cnt, bool need, float qx, float qy, float qz,
+                                           float tau, int& bc, WarpSmem& W, const float4* __restrict__ pts,
+                                           int32_t w0, int32_t w1, int lane) {
+    if (lane < cnt) W.pts[lane] = __ldg(pts + first + lane);
+    __syncwarp();
+    if (need) {
+        for (int t = 0; t < cnt; ++t) {
+            const float4 p = W.pts[t];
+            const float d = dist2(qx, qy, qz, p.x, p.y, p.z);
+            const int32_t idx = first + t;
+            if (d <= tau && (idx < w0 || idx >= w1)) {
+                W.buf[bc][lane] = pack_key(d, idx);
+                ++bc;
+            }
+        }
+    }
+    __syncwarp();
+}
 
 // ---- 3x3 symmetric eigensolver: cyclic Jacobi (Golub & Van Loan, Matrix
 // Computations, 4th ed., Alg. 8.5.2 sym.schur2 + 8.5.3), explicit indices ----
@@ -158,38 +221,104 @@ __device__ __forceinline__ void neu_add(float& s, float& c, float x) {
     s = t;
 }
 
-template <int K, bool EXACT>
-__device__ __forceinline__ void scan_bucket(int32_t first, int cnt, bool need, float qx, float qy, float qz,
-                                            TopK<K, EXACT>& tk, const float4* __restrict__ pts, int64_t w0,
-                                            int64_t w1, int lane) {
-    const float4 p = lane < cnt ? __ldg(pts + first + lane) : make_float4(0.f, 0.f, 0.f, 0.f);
-    for (int t = 0; t < cnt; ++t) {
-        const float px = __shfl_sync(FULL, p.x, t);
-        const float py = __shfl_sync(FULL, p.y, t);
-        const float pz = __shfl_sync(FULL, p.z, t);
-        const int32_t idx = first + t;
-        if (need && (idx < w0 || idx >= w1)) tk.consider(dist2(qx, qy, qz, px, py, pz), idx);
+// Normal of one query from its k neighbours (heap[0..k), ascending):
+// centred covariance with compensated FP32 sums, FP32 Jacobi, FP64 redo when
+// the relative eigengap (l1 - l0) / l2 is below `gap`, orientation towards
+// the viewpoint (src/NormalEstimation.hpp:184-189).
+template <int K>
+__device__ __forceinline__ void estimate_normal(const int32_t (&nbr)[K], int k, const float4* __restrict__ pts,
+                                                float qx, float qy, float qz, const QArgs& a, float* out,
+                                                DevState* st) {
+    float s[3] = {0.f, 0.f, 0.f}, c[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        if (j >= k) break;
+        const float4 p = __ldg(pts + nbr[j]);
+        neu_add(s[0], c[0], p.x - qx);
+        neu_add(s[1], c[1], p.y - qy);
+        neu_add(s[2], c[2], p.z - qz);
     }
+    const float inv_k = 1.0f / (float)k;
+    const float m0 = (s[0] + c[0]) * inv_k, m1 = (s[1] + c[1]) * inv_k, m2 = (s[2] + c[2]) * inv_k;
+    float cs[6] = {0, 0, 0, 0, 0, 0}, cc[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        if (j >= k) break;
+        const float4 p = __ldg(pts + nbr[j]);
+        const float r0 = (p.x - qx) - m0, r1 = (p.y - qy) - m1, r2 = (p.z - qz) - m2;
+        neu_add(cs[0], cc[0], r0 * r0);
+        neu_add(cs[1], cc[1], r0 * r1);
+        neu_add(cs[2], cc[2], r0 * r2);
+        neu_add(cs[3], cc[3], r1 * r1);
+        neu_add(cs[4], cc[4], r1 * r2);
+        neu_add(cs[5], cc[5], r2 * r2);
+    }
+    const float inv_den = 1.0f / (float)(k > 1 ? k - 1 : 1);
+    float C[6];
+#pragma unroll
+    for (int e = 0; e < 6; ++e) C[e] = (cs[e] + cc[e]) * inv_den;
+    float w[3], nv[3];
+    eig3<float>(C, w, nv);
+    float nx = nv[0], ny = nv[1], nz = nv[2];
+    const float gap = (w[1] - w[0]) / fmaxf(fabsf(w[2]), FLT_MIN);
+    if (!(gap >= a.gap)) {
+        // near-degenerate neighbourhood: redo covariance and eigensolve in FP64
+        double sd[3] = {0, 0, 0};
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            if (j >= k) break;
+            const float4 p = __ldg(pts + nbr[j]);
+            sd[0] += (double)p.x - (double)qx;
+            sd[1] += (double)p.y - (double)qy;
+            sd[2] += (double)p.z - (double)qz;
+        }
+        const double md[3] = {sd[0] / k, sd[1] / k, sd[2] / k};
+        double Cd[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            if (j >= k) break;
+            const float4 p = __ldg(pts + nbr[j]);
+            const double r0 = ((double)p.x - (double)qx) - md[0];
+            const double r1 = ((double)p.y - (double)qy) - md[1];
+            const double r2 = ((double)p.z - (double)qz) - md[2];
+            Cd[0] += r0 * r0; Cd[1] += r0 * r1; Cd[2] += r0 * r2;
+            Cd[3] += r1 * r1; Cd[4] += r1 * r2; Cd[5] += r2 * r2;
+        }
+        const double dd = (double)(k > 1 ? k - 1 : 1);
+#pragma unroll
+        for (int e = 0; e < 6; ++e) Cd[e] /= dd;
+        double wd[3], nd[3];
+        eig3<double>(Cd, wd, nd);
+        nx = (float)nd[0];
+        ny = (float)nd[1];
+        nz = (float)nd[2];
+        atomicAdd(&st->counters[CNT_FP64], 1ull);
+    }
+    const float dot = (a.vx - qx) * nx + (a.vy - qy) * ny + (a.vz - qz) * nz;
+    if (dot < 0.0f) { nx = -nx; ny = -ny; nz = -nz; }
+    out[0] = nx;
+    out[1] = ny;
+    out[2] = nz;
 }
 
 template <int K, bool EXACT, bool EXT, bool NORMALS>
 __global__ void __launch_bounds__(kKnnThreads) k_knn(const float4* __restrict__ pts, const SNode* __restrict__ snodes,
                                                      const uint64_t* __restrict__ codes, QArgs a, DevState* st) {
-    __shared__ int32_t s_stack[kKnnWarps][kStackDepth];
+    extern __shared__ __align__(16) unsigned char knn_smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    WarpSmem& W = reinterpret_cast<WarpSmem*>(knn_smem)[warp];
     const int64_t q0 = ((int64_t)blockIdx.x * kKnnWarps + warp) * 32;
     if (q0 >= a.count) return;  // whole warp
     const int64_t qo = q0 + lane;
     const bool active = qo < a.count;
     const int64_t u = a.u;
     float qx, qy, qz;
-    int64_t center;
+    int64_t center;  // tree index of the warp's first query (or its code position)
     if (EXT) {
         const int64_t src = active ? qo : q0;
         qx = __ldg(a.ext + 3 * src);
         qy = __ldg(a.ext + 3 * src + 1);
         qz = __ldg(a.ext + 3 * src + 2);
-        // seed window centre: position of the warp's first query's code
         const float lx = __shfl_sync(FULL, qx, 0), ly = __shfl_sync(FULL, qy, 0), lz = __shfl_sync(FULL, qz, 0);
         const float mn = st->min_coord, range = st->range;
         const float fbs = (float)bitscale_of(a.code_bits);
@@ -212,31 +341,48 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn(const float4* __restrict__ 
         qz = p.z;
         center = a.start + q0;
     }
-    const int64_t w0 = max64(0, center - kSeedHalo);
-    const int64_t w1 = min64(u, center + 32 + kSeedHalo);
+    const int64_t w0 = max64(0, center - a.seed_halo);
+    const int64_t w1 = min64(u, center + 32 + a.seed_halo);
+    const int S = (int)(w1 - w0);
 
     TopK<K, EXACT> tk;
     tk.init(a.k);
-    for (int64_t b = w0; b < w1; b += 32) {
-        const int cnt = (int)min64(32, w1 - b);
-        const float4 p = lane < cnt ? __ldg(pts + b + lane) : make_float4(0.f, 0.f, 0.f, 0.f);
-        for (int t = 0; t < cnt; ++t) {
-            const float px = __shfl_sync(FULL, p.x, t);
-            const float py = __shfl_sync(FULL, p.y, t);
-            const float pz = __shfl_sync(FULL, p.z, t);
-            if (active) tk.consider(dist2(qx, qy, qz, px, py, pz), (int32_t)(b + t));
+    int bc = 0;  // buffered candidates of this lane
+    Counters ct;
+
+    // Seed: each lane walks the Morton window outwards from its own position
+    // (0, +1, -1, +2, ...), so its first candidates are its index neighbours.
+    for (int i = lane; i < S; i += 32) W.pts[i] = __ldg(pts + w0 + i);
+    __syncwarp();
+    {
+        const int p = EXT ? (int)(center + 16 - w0) : (int)(center + lane - w0);
+        const int reach = max(p, S - 1 - p);
+        const int steps = 2 * (int)__reduce_max_sync(FULL, (unsigned)(active ? reach : 0)) + 1;
+        for (int t = 0; t < steps; ++t) {
+            const int off = (t & 1) ? (t + 1) >> 1 : -(t >> 1);
+            const int iw = p + off;
+            if (active && iw >= 0 && iw < S) {
+                const float4 q = W.pts[iw];
+                const float d = dist2(qx, qy, qz, q.x, q.y, q.z);
+                if (d <= tk.tau()) {
+                    W.buf[bc][lane] = pack_key(d, w0 + iw);
+                    ++bc;
+                }
+            }
+            if (t == 16 || __any_sync(FULL, bc >= kBuf)) flush(tk, bc, W, lane, ct);
         }
+        flush(tk, bc, W, lane, ct);
     }
 
     uint32_t steps = 0;
     if (u >= 2 && (w0 > 0 || w1 < u)) {
         int sp = 1;
-        if (lane == 0) s_stack[warp][0] = 0;
+        if (lane == 0) W.stack[0] = 0;
         __syncwarp();
         const uint32_t cap = (uint32_t)min64(u + 64, 0x7fffffff);
         while (sp > 0) {
             --sp;
-            const int32_t node = s_stack[warp][sp];
+            const int32_t node = W.stack[sp];
             __syncwarp();
             if (++steps > cap || node < 0 || node >= u - 1) {
                 if (lane == 0) set_err(&st->err, steps > cap ? ERRBIT_SEARCH_LIMIT : ERRBIT_BOUNDS);
@@ -245,164 +391,110 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn(const float4* __restrict__ 
             const SNode* sn = snodes + node;
             const float4 lo_l = __ldg(&sn->lo_l), hi_l = __ldg(&sn->hi_l);
             const float4 lo_r = __ldg(&sn->lo_r), hi_r = __ldg(&sn->hi_r);
-            const int32_t ref[2] = {__float_as_int(lo_l.w), __float_as_int(lo_r.w)};
-            const int32_t cnt[2] = {__float_as_int(hi_l.w), __float_as_int(hi_r.w)};
-            if (cnt[0] < 1 || cnt[1] < 1 || ref[0] < 0 || ref[1] < 0 ||
-                (cnt[0] <= a.bucket ? (int64_t)ref[0] + cnt[0] > u : ref[0] >= u - 1) ||
-                (cnt[1] <= a.bucket ? (int64_t)ref[1] + cnt[1] > u : ref[1] >= u - 1)) {
+            const int32_t refl = __float_as_int(lo_l.w), refr = __float_as_int(lo_r.w);
+            const int32_t cntl = __float_as_int(hi_l.w), cntr = __float_as_int(hi_r.w);
+            if (cntl < 1 || cntr < 1 || refl < 0 || refr < 0 ||
+                (cntl <= a.bucket ? (int64_t)refl + cntl > u : refl >= u - 1) ||
+                (cntr <= a.bucket ? (int64_t)refr + cntr > u : refr >= u - 1)) {
                 if (lane == 0) set_err(&st->err, ERRBIT_BOUNDS);
                 break;
             }
+            const float tau = tk.tau();
             const float dl = box_dist2(qx, qy, qz, lo_l.x, lo_l.y, lo_l.z, hi_l.x, hi_l.y, hi_l.z);
             const float dr = box_dist2(qx, qy, qz, lo_r.x, lo_r.y, lo_r.z, hi_r.x, hi_r.y, hi_r.z);
-            const uint32_t bl = __ballot_sync(FULL, active && dl <= tk.bd);
-            const uint32_t br = __ballot_sync(FULL, active && dr <= tk.bd);
+            const uint32_t bl = __ballot_sync(FULL, active && dl <= tau);
+            const uint32_t br = __ballot_sync(FULL, active && dr <= tau);
             if (!(bl | br)) continue;
             const uint32_t vote = __ballot_sync(FULL, active && dl <= dr);
             const int nact = __popc(__ballot_sync(FULL, active));
-            const int firstSide = (2 * __popc(vote) >= nact) ? 0 : 1;
+            const bool leftFirst = 2 * __popc(vote) >= nact;
 #pragma unroll
             for (int o = 0; o < 2; ++o) {
-                const int side = o ? 1 - firstSide : firstSide;
-                if (cnt[side] > a.bucket) continue;
-                const float ds = side ? dr : dl;
-                const bool need = active && ds <= tk.bd;
+                const bool left = (o == 0) == leftFirst;
+                const int32_t cnt = left ? cntl : cntr;
+                if (cnt > a.bucket) continue;
+                const int32_t first = left ? refl : refr;
+                if (first >= w0 && first + cnt <= w1) continue;  // all of it was in the seed window
+                const bool need = active && (left ? dl : dr) <= tk.tau();
                 if (!__ballot_sync(FULL, need)) continue;
-                scan_bucket<K, EXACT>(ref[side], cnt[side], need, qx, qy, qz, tk, pts, w0, w1, lane);
+                if (__any_sync(FULL, bc + cnt > kBuf)) flush(tk, bc, W, lane, ct);
+                ++ct.buckets;
+                scan_chunk(first, cnt, need, qx, qy, qz, tk.tau(), bc, W, pts, (int32_t)w0, (int32_t)w1, lane);
             }
 #pragma unroll
             for (int o = 1; o >= 0; --o) {
-                const int side = o ? 1 - firstSide : firstSide;
-                if (cnt[side] <= a.bucket || !(side ? br : bl)) continue;
+                const bool left = (o == 0) == leftFirst;
+                if ((left ? cntl : cntr) <= a.bucket || !(left ? bl : br)) continue;
                 if (sp >= kStackDepth) {
                     if (lane == 0) set_err(&st->err, ERRBIT_STACK);
                     continue;
                 }
-                if (lane == 0) s_stack[warp][sp] = ref[side];
+                if (lane == 0) W.stack[sp] = left ? refl : refr;
                 ++sp;
             }
             __syncwarp();
         }
     }
-    if (lane == 0 && steps) atomicAdd(&st->nodes_visited, (unsigned long long)steps);
+    flush(tk, bc, W, lane, ct);
+    {
+        const unsigned cand = __reduce_add_sync(FULL, (unsigned)ct.cand);
+        const unsigned ins = __reduce_add_sync(FULL, (unsigned)ct.ins);
+        if (lane == 0) {
+            atomicAdd(&st->counters[CNT_NODES], (unsigned long long)steps);
+            atomicAdd(&st->counters[CNT_BUCKETS], (unsigned long long)ct.buckets);
+            atomicAdd(&st->counters[CNT_MERGE], (unsigned long long)ct.merge);
+            atomicAdd(&st->counters[CNT_CANDIDATES], (unsigned long long)cand);
+            atomicAdd(&st->counters[CNT_INSERTS], (unsigned long long)ins);
+        }
+    }
     if (!active) return;
 
     // fewer than k points in the tree: repeat entry 0 (src/Octree.hpp:181-191)
+    int32_t nbr[K];
 #pragma unroll
-    for (int j = 1; j < K; ++j)
-        if (j < a.k && tk.id[j] == INT_MAX) { tk.id[j] = tk.id[0]; tk.d[j] = tk.d[0]; }
-
+    for (int j = 0; j < K; ++j) {
+        if (j > 0 && tk.key[j] == kEmptyKey) tk.key[j] = tk.key[0];
+        nbr[j] = key_idx(tk.key[j]);
+    }
     if (a.out_idx) {
         int32_t* o = a.out_idx + qo * a.k;
 #pragma unroll
         for (int j = 0; j < K; ++j)
-            if (j < a.k) o[j] = tk.id[j];
+            if (j < a.k) o[j] = nbr[j];
     }
     if (a.out_d2) {
         float* o = a.out_d2 + qo * a.k;
 #pragma unroll
         for (int j = 0; j < K; ++j)
-            if (j < a.k) o[j] = tk.d[j];
+            if (j < a.k) o[j] = key_d(tk.key[j]);
     }
-    if (NORMALS) {
-        const int k = a.k;
-        // centroid of the neighbours relative to the query, compensated sums
-        float s[3] = {0.f, 0.f, 0.f}, c[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-        for (int j = 0; j < K; ++j) {
-            if (j < k) {
-                const float4 p = __ldg(pts + tk.id[j]);
-                neu_add(s[0], c[0], p.x - qx);
-                neu_add(s[1], c[1], p.y - qy);
-                neu_add(s[2], c[2], p.z - qz);
-            }
-        }
-        const float inv_k = 1.0f / (float)k;
-        const float m0 = (s[0] + c[0]) * inv_k, m1 = (s[1] + c[1]) * inv_k, m2 = (s[2] + c[2]) * inv_k;
-        float cs[6] = {0, 0, 0, 0, 0, 0}, cc[6] = {0, 0, 0, 0, 0, 0};
-#pragma unroll
-        for (int j = 0; j < K; ++j) {
-            if (j < k) {
-                const float4 p = __ldg(pts + tk.id[j]);
-                const float r0 = (p.x - qx) - m0, r1 = (p.y - qy) - m1, r2 = (p.z - qz) - m2;
-                neu_add(cs[0], cc[0], r0 * r0);
-                neu_add(cs[1], cc[1], r0 * r1);
-                neu_add(cs[2], cc[2], r0 * r2);
-                neu_add(cs[3], cc[3], r1 * r1);
-                neu_add(cs[4], cc[4], r1 * r2);
-                neu_add(cs[5], cc[5], r2 * r2);
-            }
-        }
-        const float inv_den = 1.0f / (float)(k > 1 ? k - 1 : 1);
-        float C[6];
-#pragma unroll
-        for (int e = 0; e < 6; ++e) C[e] = (cs[e] + cc[e]) * inv_den;
-        float w[3], nv[3];
-        eig3<float>(C, w, nv);
-        float nx = nv[0], ny = nv[1], nz = nv[2];
-        const float gap = (w[1] - w[0]) / fmaxf(fabsf(w[2]), FLT_MIN);
-        if (!(gap >= a.gap)) {
-            // near-degenerate neighbourhood: redo covariance and eigensolve in FP64
-            double sd[3] = {0, 0, 0};
-#pragma unroll
-            for (int j = 0; j < K; ++j) {
-                if (j < k) {
-                    const float4 p = __ldg(pts + tk.id[j]);
-                    sd[0] += (double)p.x - (double)qx;
-                    sd[1] += (double)p.y - (double)qy;
-                    sd[2] += (double)p.z - (double)qz;
-                }
-            }
-            const double md[3] = {sd[0] / k, sd[1] / k, sd[2] / k};
-            double Cd[6] = {0, 0, 0, 0, 0, 0};
-#pragma unroll
-            for (int j = 0; j < K; ++j) {
-                if (j < k) {
-                    const float4 p = __ldg(pts + tk.id[j]);
-                    const double r0 = ((double)p.x - (double)qx) - md[0];
-                    const double r1 = ((double)p.y - (double)qy) - md[1];
-                    const double r2 = ((double)p.z - (double)qz) - md[2];
-                    Cd[0] += r0 * r0; Cd[1] += r0 * r1; Cd[2] += r0 * r2;
-                    Cd[3] += r1 * r1; Cd[4] += r1 * r2; Cd[5] += r2 * r2;
-                }
-            }
-            const double dd = (double)(k > 1 ? k - 1 : 1);
-#pragma unroll
-            for (int e = 0; e < 6; ++e) Cd[e] /= dd;
-            double wd[3], nd[3];
-            eig3<double>(Cd, wd, nd);
-            nx = (float)nd[0];
-            ny = (float)nd[1];
-            nz = (float)nd[2];
-            atomicAdd(&st->fp64_solves, 1ull);
-        }
-        // orientation towards the viewpoint (src/NormalEstimation.hpp:184-189)
-        const float dot = (a.vx - qx) * nx + (a.vy - qy) * ny + (a.vz - qz) * nz;
-        if (dot < 0.0f) { nx = -nx; ny = -ny; nz = -nz; }
-        float* o = a.out_normals + 3 * qo;
-        o[0] = nx;
-        o[1] = ny;
-        o[2] = nz;
-    }
+    if (NORMALS) estimate_normal<K>(nbr, a.k, pts, qx, qy, qz, a, a.out_normals + 3 * qo, st);
+}
+
+template <int K, bool EXACT, bool EXT, bool NORMALS>
+cudaError_t launch_one(const BuildBufs& b, const QArgs& a, unsigned blocks, cudaStream_t s) {
+    constexpr int smem = (int)sizeof(WarpSmem) * kKnnWarps;
+    cudaError_t e =
+        cudaFuncSetAttribute(k_knn<K, EXACT, EXT, NORMALS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    k_knn<K, EXACT, EXT, NORMALS><<<blocks, kKnnThreads, smem, s>>>(b.pts4, b.snodes, b.codes, a, b.st);
+    return cudaGetLastError();
 }
 
 template <int K, bool EXACT>
 cudaError_t launch_k(const BuildBufs& b, const QArgs& a, bool ext, bool normals, cudaStream_t s) {
     const int64_t warps = (a.count + 31) / 32;
     const unsigned blocks = (unsigned)((warps + kKnnWarps - 1) / kKnnWarps);
-    if (ext)
-        k_knn<K, EXACT, true, false><<<blocks, kKnnThreads, 0, s>>>(b.pts4, b.snodes, b.codes, a, b.st);
-    else if (normals)
-        k_knn<K, EXACT, false, true><<<blocks, kKnnThreads, 0, s>>>(b.pts4, b.snodes, b.codes, a, b.st);
-    else
-        k_knn<K, EXACT, false, false><<<blocks, kKnnThreads, 0, s>>>(b.pts4, b.snodes, b.codes, a, b.st);
-    return cudaGetLastError();
+    if (ext) return launch_one<K, EXACT, true, false>(b, a, blocks, s);
+    if (normals) return launch_one<K, EXACT, false, true>(b, a, blocks, s);
+    return launch_one<K, EXACT, false, false>(b, a, blocks, s);
 }
 
 }  // namespace
 
 cudaError_t enqueue_query(const BuildBufs& b, const QueryParams& q, cudaStream_t s, int /*num_sms*/) {
     if (q.count <= 0) return cudaSuccess;
+    if (q.k < 1 || q.k > 32) return cudaErrorInvalidValue;
     QArgs a;
     a.k = q.k;
     a.start = q.start;
@@ -418,6 +510,9 @@ cudaError_t enqueue_query(const BuildBufs& b, const QueryParams& q, cudaStream_t
     a.gap = q.eigengap_fp64;
     a.code_bits = q.code_bits;
     a.bucket = q.bucket;
+    a.seed_halo = q.seed_halo;
+    if (a.seed_halo > kMaxHalo) a.seed_halo = kMaxHalo;
+    if (a.seed_halo < 0) a.seed_halo = 0;
     const bool ext = q.ext_queries != nullptr;
     const bool nrm = q.out_normals != nullptr && !ext;
     switch (q.k) {
@@ -427,7 +522,6 @@ cudaError_t enqueue_query(const BuildBufs& b, const QueryParams& q, cudaStream_t
         case 32: return launch_k<32, true>(b, a, ext, nrm, s);
         default: break;
     }
-    if (q.k < 1 || q.k > 32) return cudaErrorInvalidValue;
     if (q.k <= 4) return launch_k<4, false>(b, a, ext, nrm, s);
     if (q.k <= 8) return launch_k<8, false>(b, a, ext, nrm, s);
     if (q.k <= 12) return launch_k<12, false>(b, a, ext, nrm, s);

@@ -19,6 +19,10 @@ constexpr int kScanThreads = 256;
 constexpr int kScanIpt = 16;
 constexpr int kScanTile = kScanThreads * kScanIpt;
 
+// Query counters: fp64 solves, nodes visited, buckets scanned, candidates,
+// merge steps, inserts.
+enum { CNT_FP64 = 0, CNT_NODES, CNT_BUCKETS, CNT_CANDIDATES, CNT_MERGE, CNT_INSERTS, kQueryCounters };
+
 // Small device-resident state of one build (zeroed at the start of each build).
 struct DevState {
     uint32_t err;
@@ -38,8 +42,8 @@ struct DevState {
     // fixed-root description used by the search hierarchy (node 0)
     int32_t sroot_gamma;
     int32_t sroot_hl, sroot_hr;
-    unsigned long long fp64_solves;
-    unsigned long long nodes_visited;
+    // query counters, in the order of se_stats
+    unsigned long long counters[kQueryCounters];
 };
 
 // Byte layout of OT::OTNode (reference src/Octree.hpp:19-36), 56 bytes.
@@ -129,6 +133,7 @@ struct QueryParams {
     float eigengap_fp64;
     int code_bits;
     int bucket;
+    int seed_halo;
 };
 
 cudaError_t enqueue_query(const BuildBufs& b, const QueryParams& q, cudaStream_t s, int num_sms);
