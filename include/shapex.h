@@ -171,6 +171,27 @@ typedef struct se_profile {
 } se_profile;
 int se_get_profile(se_ctx* ctx, se_profile* prof);
 
+/* Sorts n 64-bit keys (e.g. Morton codes) ascending on the current device
+ * WITHOUT ALLOCATING. It has no counterpart in the reference.
+ * For callers that cannot call cudaMalloc: code running inside another
+ * framework's memory budget (the host application owns all device memory) and
+ * latency-critical loops where cudaMalloc/cudaFree, which can synchronise the
+ * device, are not allowed. d_keys_in and d_keys_out are caller-owned device
+ * arrays of n keys (they may be the same array); every other byte it needs is
+ * one file-scope static device array inside the library (SE_STATIC_SORT_BYTES
+ * on every GPU that loads the library, held until the process exits).
+ * - n may not exceed SE_STATIC_SORT_MAX_KEYS: larger n returns
+ *   SE_ERR_INVALID_ARG and touches nothing.
+ * - The first call on a device looks up the scratch's device address; make
+ *   that first call before any stream capture on that device.
+ * - All calls on one device share the scratch: calls that overlap on the GPU
+ *   (different streams or host threads, without ordering) race on it.
+ * - Runs on `stream` (a cudaStream_t, NULL for the legacy default stream) and
+ *   returns after the sort has finished. */
+#define SE_STATIC_SORT_MAX_KEYS (1 << 20)
+#define SE_STATIC_SORT_BYTES (8u * (1u << 20) + 256u * 1024u + 20480u)
+int se_sort_keys_static(const uint64_t* d_keys_in, uint64_t* d_keys_out, int64_t n, void* stream);
+
 /* Waits for all work queued on the context's stream. */
 int se_synchronize(se_ctx* ctx);
 

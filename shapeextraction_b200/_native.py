@@ -29,6 +29,7 @@ EXPORTS = [
     "se_options_init", "se_status_string", "se_abi_version", "se_create", "se_destroy", "se_last_error",
     "se_build", "se_get_info", "se_get_device_views", "se_get_codes", "se_get_radix", "se_get_octree",
     "se_get_points", "se_knn_self", "se_knn", "se_normals", "se_get_stats", "se_get_profile", "se_synchronize",
+    "se_sort_keys_static",
 ]
 
 OTNODE_DTYPE = np.dtype([
@@ -112,6 +113,7 @@ def lib():
             "se_get_stats": (i32, [P, ctypes.POINTER(SeStats)]),
             "se_get_profile": (i32, [P, ctypes.POINTER(SeProfile)]),
             "se_synchronize": (i32, [P]),
+            "se_sort_keys_static": (i32, [P, P, i64, P]),
         }
         for name, (res, args) in sigs.items():
             fn = getattr(L, name)

@@ -747,6 +747,34 @@ __global__ void __launch_bounds__(256) k_oct_link(OtNode* __restrict__ nodes, in
     }
 }
 
+// Digit histograms of given keys (the histogram half of k_encode), for
+// sorting keys that were not produced by k_encode.
+__global__ void __launch_bounds__(256) k_hist_keys(const uint64_t* __restrict__ keys, int64_t n, DevState* st) {
+    __shared__ uint32_t s_h[kSortPasses][256];
+    for (int i = threadIdx.x; i < kSortPasses * 256; i += blockDim.x) (&s_h[0][0])[i] = 0;
+    __syncthreads();
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint64_t c = keys[i];
+#pragma unroll
+        for (int p = 0; p < kSortPasses; ++p) atomicAdd(&s_h[p][(c >> (8 * p)) & 255], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kSortPasses * 256; i += blockDim.x) {
+        const uint32_t v = (&s_h[0][0])[i];
+        if (v) atomicAdd(&(&st->hist[0][0])[i], v);
+    }
+}
+
+// After the sort passes the result sits in buf1 when an odd number of passes
+// ran; copy it back into buf0.
+__global__ void __launch_bounds__(256) k_copy_if_odd(const uint64_t* __restrict__ src, uint64_t* __restrict__ dst,
+                                                     int64_t n, const DevState* st) {
+    if (!(st->n_active & 1)) return;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) dst[i] = src[i];
+}
+
 inline unsigned grid_for(int64_t work, int threads, int64_t cap_blocks) {
     int64_t b = (work + threads - 1) / threads;
     if (b < 1) b = 1;
@@ -755,6 +783,24 @@ inline unsigned grid_for(int64_t work, int threads, int64_t cap_blocks) {
 }
 
 }  // namespace
+
+cudaError_t enqueue_sort_keys(uint64_t* keys, uint64_t* tmp, int64_t n, uint32_t* lookback, DevState* st,
+                              cudaStream_t s, int num_sms) {
+    cudaError_t e = cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sizeof(SortSmem));
+    if (e != cudaSuccess) return e;
+    cudaMemsetAsync(st, 0, sizeof(DevState), s);
+    if (n <= 0) return cudaGetLastError();
+    k_hist_keys<<<grid_for(n, 256, num_sms * 4), 256, 0, s>>>(keys, n, st);
+    k_sort_prep<<<1, 256, 0, s>>>(n, st);
+    const int64_t sort_tiles = (n + kSortTile - 1) / kSortTile;
+    for (int pass = 0; pass < kSortPasses; ++pass) {
+        cudaMemsetAsync(lookback, 0, sizeof(uint32_t) * 256 * sort_tiles, s);
+        k_onesweep<<<(unsigned)sort_tiles, kSortThreads, sizeof(SortSmem), s>>>(keys, tmp, n, pass, lookback, st);
+    }
+    k_copy_if_odd<<<grid_for(n, 256, num_sms * 4), 256, 0, s>>>(tmp, keys, n, st);
+    return cudaGetLastError();
+}
 
 cudaError_t enqueue_octree(const BuildBufs& b, const BuildParams& p, cudaStream_t s, int num_sms, int* launches) {
     const int64_t n = p.n;

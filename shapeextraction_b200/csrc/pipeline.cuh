@@ -120,6 +120,11 @@ cudaError_t enqueue_build(const BuildBufs& b, const BuildParams& p, cudaStream_t
 // Enqueue only the octree stage (used to redo it after a capacity regrow).
 cudaError_t enqueue_octree(const BuildBufs& b, const BuildParams& p, cudaStream_t s, int num_sms, int* launches);
 
+// Sort n 64-bit keys in place in `keys` (ascending) with the onesweep passes;
+// `tmp` (n keys), `lookback` (256 words per 4096-key tile) and `st` are scratch.
+cudaError_t enqueue_sort_keys(uint64_t* keys, uint64_t* tmp, int64_t n, uint32_t* lookback, DevState* st,
+                              cudaStream_t s, int num_sms);
+
 struct QueryParams {
     int k;
     int64_t start;      // first query (self queries)
