@@ -35,7 +35,7 @@ namespace {
 constexpr int kKnnThreads = 128;
 constexpr int kKnnWarps = kKnnThreads / 32;
 constexpr int kStackDepth = 96;
-constexpr int kBuf = 32;                // per-lane candidate buffer slots
+constexpr int kBuf = 64;                // per-lane candidate buffer slots (point indices)
 constexpr int kMaxHalo = 48;            // seed points on each side of a warp's queries
 constexpr int kWindowMax = 32 + 2 * kMaxHalo;
 constexpr unsigned FULL = 0xffffffffu;
@@ -65,6 +65,27 @@ struct TopK {
         kk = k;
     }
     __device__ __forceinline__ float tau() const { return key_d(bk); }
+    // After key[0..K) was filled with arbitrary keys: sort ascending with an
+    // odd-even transposition network (K passes of independent
+    // compare-exchanges) and set the bound.
+    __device__ __forceinline__ void sort_filled() {
+#pragma unroll
+        for (int pass = 0; pass < K; ++pass) {
+#pragma unroll
+            for (int j = pass & 1; j + 1 < K; j += 2) {
+                const unsigned long long a = key[j], b = key[j + 1];
+                key[j] = a < b ? a : b;
+                key[j + 1] = a < b ? b : a;
+            }
+        }
+        if (EXACT) {
+            bk = key[K - 1];
+        } else {
+#pragma unroll
+            for (int j = 0; j < K; ++j)
+                if (j == kk - 1) bk = key[j];
+        }
+    }
     __device__ __forceinline__ void insert(unsigned long long nk) {  // requires nk < bk
         bool lt[K];
 #pragma unroll
@@ -87,7 +108,7 @@ struct TopK {
 struct WarpSmem {
     int32_t stack[kStackDepth];
     float4 pts[kWindowMax];
-    unsigned long long buf[kBuf][32];
+    int32_t buf[kBuf][32];
 };
 
 struct QArgs {
@@ -111,13 +132,16 @@ struct Counters {
 // Merge every lane's buffered candidates into its list; the warp steps
 // through max-over-lanes slots together.
 template <int K, bool EXACT>
-__device__ __forceinline__ void flush(TopK<K, EXACT>& tk, int& bc, WarpSmem& W, int lane, Counters& ct) {
+__device__ __forceinline__ void flush(TopK<K, EXACT>& tk, int& bc, WarpSmem& W, int lane, Counters& ct,
+                                      const float4* __restrict__ pts, float qx, float qy, float qz) {
     const int maxc = (int)__reduce_max_sync(FULL, (unsigned)bc);
     ct.merge += maxc;
     ct.cand += bc;
     for (int j = 0; j < maxc; ++j) {
         if (j < bc) {
-            const unsigned long long nk = W.buf[j][lane];
+            const int32_t idx = W.buf[j][lane];
+            const float4 p = __ldg(pts + idx);
+            const unsigned long long nk = pack_key(dist2(qx, qy, qz, p.x, p.y, p.z), idx);
             if (nk < tk.bk) {
                 tk.insert(nk);
                 ++ct.ins;
@@ -137,15 +161,43 @@ __device__ __forceinline__ void scan_chunk(int32_t first, int cnt, bool need, fl
     if (lane < cnt) W.pts[lane] = __ldg(pts + first + lane);
     __syncwarp();
     if (need) {
-        for (int t = 0; t < cnt; ++t) {
-            const float4 p = W.pts[t];
-            const float d = dist2(qx, qy, qz, p.x, p.y, p.z);
-            const int32_t idx = first + t;
-            if (d <= tau && (idx < w0 || idx >= w1)) {
-                W.buf[bc][lane] = pack_key(d, idx);
-                ++bc;
+        if (first < w1 && first + cnt > w0) {  // overlaps the seed window: skip its points
+            for (int t = 0; t < cnt; ++t) {
+                const float4 p = W.pts[t];
+                const float d = dist2(qx, qy, qz, p.x, p.y, p.z);
+                const int32_t idx = first + t;
+                if (d <= tau && (idx < w0 || idx >= w1)) W.buf[bc++][lane] = idx;
+            }
+        } else {
+            for (int t = 0; t < cnt; ++t) {
+                const float4 p = W.pts[t];
+                if (dist2(qx, qy, qz, p.x, p.y, p.z) <= tau) W.buf[bc++][lane] = first + t;
             }
         }
+    }
+    __syncwarp();
+}
+
+// Same as scan_chunk when few lanes need the bucket (`mask`): each lane holds
+// one point of the bucket and the warp steps over the needing queries, so the
+// cost follows the number of needing lanes rather than the bucket size. Hits
+// are appended to the needing lane's buffer in ballot order.
+__device__ __forceinline__ void scan_sparse(int32_t first, int cnt, uint32_t mask, float qx, float qy, float qz,
+                                            float tau, int& bc, WarpSmem& W, const float4* __restrict__ pts,
+                                            int32_t w0, int32_t w1, int lane) {
+    const int32_t idx = first + lane;
+    const bool has = lane < cnt && (idx < w0 || idx >= w1);
+    const float4 p = lane < cnt ? __ldg(pts + idx) : make_float4(0.f, 0.f, 0.f, 0.f);
+    while (mask) {
+        const int i = __ffs(mask) - 1;
+        mask &= mask - 1;
+        const float xi = __shfl_sync(FULL, qx, i), yi = __shfl_sync(FULL, qy, i), zi = __shfl_sync(FULL, qz, i);
+        const float ti = __shfl_sync(FULL, tau, i);
+        const int base = __shfl_sync(FULL, bc, i);
+        const bool pass = has && dist2(xi, yi, zi, p.x, p.y, p.z) <= ti;
+        const uint32_t pm = __ballot_sync(FULL, pass);
+        if (pass) W.buf[base + __popc(pm & lanemask_lt())][i] = idx;
+        if (lane == i) bc += __popc(pm);
     }
     __syncwarp();
 }
@@ -358,20 +410,33 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn(const float4* __restrict__ 
         const int p = EXT ? (int)(center + 16 - w0) : (int)(center + lane - w0);
         const int reach = max(p, S - 1 - p);
         const int steps = 2 * (int)__reduce_max_sync(FULL, (unsigned)(active ? reach : 0)) + 1;
-        for (int t = 0; t < steps; ++t) {
+        // the first K spiral candidates fill the list directly, then one sort
+#pragma unroll
+        for (int t = 0; t < K; ++t) {
+            const int off = (t & 1) ? (t + 1) >> 1 : -(t >> 1);
+            const int iw = p + off;
+            unsigned long long kv = kEmptyKey;
+            if (active && iw >= 0 && iw < S) {
+                const float4 q = W.pts[iw];
+                kv = pack_key(dist2(qx, qy, qz, q.x, q.y, q.z), w0 + iw);
+            }
+            tk.key[t] = kv;
+        }
+        tk.sort_filled();
+        float tau = tk.tau();
+        for (int t = K; t < steps; ++t) {
             const int off = (t & 1) ? (t + 1) >> 1 : -(t >> 1);
             const int iw = p + off;
             if (active && iw >= 0 && iw < S) {
                 const float4 q = W.pts[iw];
-                const float d = dist2(qx, qy, qz, q.x, q.y, q.z);
-                if (d <= tk.tau()) {
-                    W.buf[bc][lane] = pack_key(d, w0 + iw);
-                    ++bc;
-                }
+                if (dist2(qx, qy, qz, q.x, q.y, q.z) <= tau) W.buf[bc++][lane] = (int32_t)(w0 + iw);
             }
-            if (t == 16 || __any_sync(FULL, bc >= kBuf)) flush(tk, bc, W, lane, ct);
+            if (__any_sync(FULL, bc == kBuf)) {
+                flush(tk, bc, W, lane, ct, pts, qx, qy, qz);
+                tau = tk.tau();
+            }
         }
-        flush(tk, bc, W, lane, ct);
+        flush(tk, bc, W, lane, ct, pts, qx, qy, qz);
     }
 
     uint32_t steps = 0;
@@ -393,9 +458,12 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn(const float4* __restrict__ 
             const float4 lo_r = __ldg(&sn->lo_r), hi_r = __ldg(&sn->hi_r);
             const int32_t refl = __float_as_int(lo_l.w), refr = __float_as_int(lo_r.w);
             const int32_t cntl = __float_as_int(hi_l.w), cntr = __float_as_int(hi_r.w);
-            if (cntl < 1 || cntr < 1 || refl < 0 || refr < 0 ||
-                (cntl <= a.bucket ? (int64_t)refl + cntl > u : refl >= u - 1) ||
-                (cntr <= a.bucket ? (int64_t)refr + cntr > u : refr >= u - 1)) {
+            const uint32_t u32 = (uint32_t)u;
+            const bool okl = cntl <= a.bucket ? (cntl >= 1 && (uint32_t)refl <= u32 - (uint32_t)cntl)
+                                              : (uint32_t)refl < u32 - 1;
+            const bool okr = cntr <= a.bucket ? (cntr >= 1 && (uint32_t)refr <= u32 - (uint32_t)cntr)
+                                              : (uint32_t)refr < u32 - 1;
+            if (!(okl && okr)) {
                 if (lane == 0) set_err(&st->err, ERRBIT_BOUNDS);
                 break;
             }
@@ -416,10 +484,14 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn(const float4* __restrict__ 
                 const int32_t first = left ? refl : refr;
                 if (first >= w0 && first + cnt <= w1) continue;  // all of it was in the seed window
                 const bool need = active && (left ? dl : dr) <= tk.tau();
-                if (!__ballot_sync(FULL, need)) continue;
-                if (__any_sync(FULL, bc + cnt > kBuf)) flush(tk, bc, W, lane, ct);
+                const uint32_t needm = __ballot_sync(FULL, need);
+                if (!needm) continue;
+                if (__any_sync(FULL, bc + cnt > kBuf)) flush(tk, bc, W, lane, ct, pts, qx, qy, qz);
                 ++ct.buckets;
-                scan_chunk(first, cnt, need, qx, qy, qz, tk.tau(), bc, W, pts, (int32_t)w0, (int32_t)w1, lane);
+                if (3 * __popc(needm) < 2 * cnt)
+                    scan_sparse(first, cnt, needm, qx, qy, qz, tk.tau(), bc, W, pts, (int32_t)w0, (int32_t)w1, lane);
+                else
+                    scan_chunk(first, cnt, need, qx, qy, qz, tk.tau(), bc, W, pts, (int32_t)w0, (int32_t)w1, lane);
             }
 #pragma unroll
             for (int o = 1; o >= 0; --o) {
@@ -435,7 +507,7 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn(const float4* __restrict__ 
             __syncwarp();
         }
     }
-    flush(tk, bc, W, lane, ct);
+    flush(tk, bc, W, lane, ct, pts, qx, qy, qz);
     {
         const unsigned cand = __reduce_add_sync(FULL, (unsigned)ct.cand);
         const unsigned ins = __reduce_add_sync(FULL, (unsigned)ct.ins);
