@@ -55,7 +55,10 @@ typedef struct se_options {
     void* stream;          /* cudaStream_t to use; NULL: the context creates one */
     int32_t seed_halo;     /* kNN: points offered on each side of a warp's 32 queries
                               before the tree walk (0..48; -1 = default) */
-    int32_t reserved[7];
+    int32_t learned;       /* 1: queries start from the learned radius (se_mlp_*);
+                              queries it underestimates are searched again without it */
+    int32_t learned_skip_seed; /* with learned: skip the Morton-window seed */
+    int32_t reserved[5];
 } se_options;
 
 /* Sizes after se_build (RT::RadixTree / OT::Octree public fields). */
@@ -156,6 +159,7 @@ typedef struct se_stats {
     int64_t candidates;      /* points that reached a query's bound, summed over queries */
     int64_t merge_steps;     /* candidate-buffer merge steps, summed over warps */
     int64_t inserts;         /* insertions into the k-best lists, summed over queries */
+    int64_t learned_misses;  /* queries whose learned radius was too small (searched again) */
 } se_stats;
 int se_get_stats(const se_ctx* ctx, se_stats* stats);
 
@@ -170,6 +174,41 @@ typedef struct se_profile {
     int32_t query_launches;
 } se_profile;
 int se_get_profile(se_ctx* ctx, se_profile* prof);
+
+/* ---- Learned search radius. No counterpart in the reference (the north
+ * star's learned stage): a 32 -> 64 -> 64 -> 1 MLP with BF16 weights and FP32
+ * accumulation predicts, per tree point, y = log2(r_k^2 / range^2) from
+ * occupancy features of the built tree; the search starts from
+ * r^2 = range^2 * 2^(y + margin) and stays exact (queries it underestimates
+ * are searched again without it). Parameters live in the context. */
+#define SE_MLP_FEATURES 32
+#define SE_MLP_PARAMS 6337
+/* Features of tree points [start, start+count): count x SE_MLP_FEATURES floats. */
+int se_features(se_ctx* ctx, int64_t start, int64_t count, float* out, int mem);
+/* Random initialisation (uniform He scaling), biases zero. */
+int se_mlp_init(se_ctx* ctx, uint64_t seed);
+/* Copy the FP32 master parameters out (set = 0) or in (set = 1). */
+int se_mlp_params(se_ctx* ctx, float* params, int set, int mem);
+/* Turn the learned starting bound on/off for later queries (se_options.learned
+ * and .learned_skip_seed at run time). */
+int se_mlp_enable(se_ctx* ctx, int learned, int skip_seed);
+/* Log-margin added to predictions to make them upper bounds. */
+int se_mlp_set_margin(se_ctx* ctx, float margin_log2);
+/* Forward pass of the training path (CUDA cores): out[n] = y-hat. */
+int se_mlp_forward(se_ctx* ctx, const float* features, int64_t n, float* out, int mem);
+/* Tensor-core inference fused with the features, on tree points
+ * [start, start+count): y-hat and/or the search bound r^2 (either may be NULL). */
+int se_mlp_predict(se_ctx* ctx, int64_t start, int64_t count, float* yhat, float* r2, int mem);
+/* Mean squared error and its gradient w.r.t. every parameter (SE_MLP_PARAMS floats). */
+int se_mlp_grad(se_ctx* ctx, const float* features, const float* targets, int64_t n, float* grads, float* loss,
+                int mem);
+/* Adam on the MSE over `steps` consecutive mini-batches of `batch` rows
+ * (cycling over the n rows); losses (optional, `steps` floats) per step. */
+int se_mlp_train(se_ctx* ctx, const float* features, const float* targets, int64_t n, int steps, int batch, float lr,
+                 float* losses, int mem);
+/* Parameters + margin to / from a file (magic "SXMLP1", F, H, params, margin). */
+int se_mlp_save(se_ctx* ctx, const char* path);
+int se_mlp_load(se_ctx* ctx, const char* path);
 
 /* Sorts n 64-bit keys (e.g. Morton codes) ascending on the current device
  * WITHOUT ALLOCATING. It has no counterpart in the reference.

@@ -799,6 +799,94 @@ int64_t or_pipeline_reference(const float* x, const float* y, const float* z, in
     return u;
 }
 
+// ---- learned-radius MLP (no counterpart in the reference) --------------------
+// 32 -> 64 -> 64 -> 1, ReLU, parameters flat as W1[32][64], b1[64],
+// W2[64][64], b2[64], w3[64], b3. With round_bf16 = 1 the forward pass
+// reproduces the GPU training kernels bit for bit: inputs, weights and hidden
+// activations rounded to BF16 (round to nearest even), FP32 fmaf accumulation
+// in the same order. Gradients of mean((yhat - y)^2) are accumulated in
+// double, treating the BF16 roundings as identity (straight-through), as the
+// GPU backward does. With round_bf16 = 0 everything is plain double math (for
+// finite-difference checks of the backward formulas).
+static float bf16_round(float v) {
+    uint32_t b;
+    std::memcpy(&b, &v, 4);
+    if ((b & 0x7f800000u) == 0x7f800000u) return v;  // inf / nan
+    b += 0x7fffu + ((b >> 16) & 1u);
+    b &= 0xffff0000u;
+    float r;
+    std::memcpy(&r, &b, 4);
+    return r;
+}
+
+int or_mlp_grad(const float* params, const float* X, const float* y, int64_t n, int round_bf16, double* yhat_out,
+                double* grads, double* loss_out) {
+    constexpr int F = 32, H = 64;
+    constexpr int W1 = 0, B1 = W1 + F * H, W2 = B1 + H, B2 = W2 + H * H, W3 = B2 + H, B3 = W3 + H, NP = B3 + 1;
+    std::vector<double> g(NP, 0.0);
+    double loss = 0.0;
+    auto rw = [&](int i) { return round_bf16 ? (double)bf16_round(params[i]) : (double)params[i]; };
+    for (int64_t r = 0; r < n; ++r) {
+        double x[F], h1[H], h2[H];
+        for (int j = 0; j < F; ++j) x[j] = round_bf16 ? (double)bf16_round(X[r * F + j]) : (double)X[r * F + j];
+        for (int i = 0; i < H; ++i) {
+            if (round_bf16) {
+                float a = params[B1 + i];
+                for (int j = 0; j < F; ++j) a = std::fmaf((float)x[j], (float)rw(W1 + j * H + i), a);
+                h1[i] = (double)bf16_round(std::fmax(a, 0.0f));
+            } else {
+                double a = params[B1 + i];
+                for (int j = 0; j < F; ++j) a += x[j] * rw(W1 + j * H + i);
+                h1[i] = a > 0 ? a : 0.0;
+            }
+        }
+        double yh;
+        if (round_bf16) {
+            float yy = params[B3];
+            for (int i = 0; i < H; ++i) {
+                float a = params[B2 + i];
+                for (int j = 0; j < H; ++j) a = std::fmaf((float)h1[j], (float)rw(W2 + j * H + i), a);
+                h2[i] = (double)bf16_round(std::fmax(a, 0.0f));
+                yy = std::fmaf((float)h2[i], (float)rw(W3 + i), yy);
+            }
+            yh = yy;
+        } else {
+            yh = params[B3];
+            for (int i = 0; i < H; ++i) {
+                double a = params[B2 + i];
+                for (int j = 0; j < H; ++j) a += h1[j] * rw(W2 + j * H + i);
+                h2[i] = a > 0 ? a : 0.0;
+                yh += h2[i] * rw(W3 + i);
+            }
+        }
+        if (yhat_out) yhat_out[r] = yh;
+        const double e = yh - (double)y[r];
+        loss += e * e / (double)n;
+        const double dy = 2.0 * e / (double)n;
+        g[B3] += dy;
+        double dh2[H], dh1[H];
+        for (int i = 0; i < H; ++i) {
+            g[W3 + i] += dy * h2[i];
+            dh2[i] = h2[i] > 0 ? dy * rw(W3 + i) : 0.0;
+            g[B2 + i] += dh2[i];
+        }
+        for (int j = 0; j < H; ++j) {
+            double a = 0.0;
+            for (int i = 0; i < H; ++i) {
+                g[W2 + j * H + i] += h1[j] * dh2[i];
+                a += rw(W2 + j * H + i) * dh2[i];
+            }
+            dh1[j] = h1[j] > 0 ? a : 0.0;
+            g[B1 + j] += dh1[j];
+        }
+        for (int f = 0; f < F; ++f)
+            for (int i = 0; i < H; ++i) g[W1 + f * H + i] += x[f] * dh1[i];
+    }
+    if (grads) std::copy(g.begin(), g.end(), grads);
+    if (loss_out) *loss_out = loss;
+    return NP;
+}
+
 // Cross-checks of the octree, after checkTree src/Octree.cu:163-177:
 // every leaf's code prefix matches its slot path, and every leaf index in
 // [0, u) appears exactly once. Returns 0 on success, else a negative code;

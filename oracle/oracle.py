@@ -60,6 +60,7 @@ def lib():
             "or_cov_ref_f32": (None, [P, P, i64, i32, P]),
             "or_octree_check": (i32, [P, i64, P, i64, i32, i32, P]),
             "or_pipeline_reference": (i64, [P, P, P, i64, i32, P]),
+            "or_mlp_grad": (i32, [P, P, P, i64, i32, P, P, P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(_lib, name)
@@ -205,6 +206,22 @@ def pipeline_reference(x, y, z, k):
     out = np.zeros((x.size, 3), np.float32)
     u = lib().or_pipeline_reference(_p(x), _p(y), _p(z), x.size, k, _p(out))
     return int(u), out[:u]
+
+
+MLP_PARAMS = 6337
+
+
+def mlp_grad(params, X, y, round_bf16=True):
+    """(yhat, loss, grads) of the learned-radius MLP's mean squared error."""
+    params = _f32(params)
+    X = _f32(X)
+    y = _f32(y)
+    n = X.shape[0]
+    yhat = np.zeros(n, np.float64)
+    grads = np.zeros(MLP_PARAMS, np.float64)
+    loss = np.zeros(1, np.float64)
+    lib().or_mlp_grad(_p(params), _p(X), _p(y), n, int(bool(round_bf16)), _p(yhat), _p(grads), _p(loss))
+    return yhat, float(loss[0]), grads
 
 
 def exact_normals(pts, k, viewpoint=(0.0, 0.0, 0.0)):

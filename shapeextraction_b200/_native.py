@@ -29,8 +29,11 @@ EXPORTS = [
     "se_options_init", "se_status_string", "se_abi_version", "se_create", "se_destroy", "se_last_error",
     "se_build", "se_get_info", "se_get_device_views", "se_get_codes", "se_get_radix", "se_get_octree",
     "se_get_points", "se_knn_self", "se_knn", "se_normals", "se_get_stats", "se_get_profile", "se_synchronize",
-    "se_sort_keys_static",
+    "se_sort_keys_static", "se_features", "se_mlp_init", "se_mlp_params", "se_mlp_enable", "se_mlp_set_margin", "se_mlp_forward",
+    "se_mlp_predict", "se_mlp_grad", "se_mlp_train", "se_mlp_save", "se_mlp_load",
 ]
+MLP_FEATURES = 32
+MLP_PARAMS = 6337
 
 OTNODE_DTYPE = np.dtype([
     ("children", "<i4", (8,)), ("corner", "<f4", (3,)), ("cell_size", "<f4"),
@@ -43,7 +46,7 @@ class SeOptions(ctypes.Structure):
         ("code_bits", ctypes.c_int32), ("root_compat", ctypes.c_int32), ("build_octree", ctypes.c_int32),
         ("viewpoint", ctypes.c_float * 3), ("eigengap_fp64", ctypes.c_float), ("leaf_bucket", ctypes.c_int32),
         ("device", ctypes.c_int32), ("stream", ctypes.c_void_p), ("seed_halo", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 7),
+        ("learned", ctypes.c_int32), ("learned_skip_seed", ctypes.c_int32), ("reserved", ctypes.c_int32 * 5),
     ]
 
 
@@ -60,7 +63,8 @@ class SeDeviceViews(ctypes.Structure):
         "codes", "points", "octree", "left_child", "parent", "prefix_n", "has_leaf_left", "has_leaf_right")]
 
 
-STAT_NAMES = ["fp64_solves", "nodes_visited", "buckets_scanned", "candidates", "merge_steps", "inserts"]
+STAT_NAMES = ["fp64_solves", "nodes_visited", "buckets_scanned", "candidates", "merge_steps", "inserts",
+              "learned_misses"]
 
 
 class SeStats(ctypes.Structure):
@@ -114,6 +118,17 @@ def lib():
             "se_get_profile": (i32, [P, ctypes.POINTER(SeProfile)]),
             "se_synchronize": (i32, [P]),
             "se_sort_keys_static": (i32, [P, P, i64, P]),
+            "se_features": (i32, [P, i64, i64, P, i32]),
+            "se_mlp_init": (i32, [P, ctypes.c_uint64]),
+            "se_mlp_params": (i32, [P, P, i32, i32]),
+            "se_mlp_enable": (i32, [P, i32, i32]),
+            "se_mlp_set_margin": (i32, [P, ctypes.c_float]),
+            "se_mlp_forward": (i32, [P, P, i64, P, i32]),
+            "se_mlp_predict": (i32, [P, i64, i64, P, P, i32]),
+            "se_mlp_grad": (i32, [P, P, P, i64, P, P, i32]),
+            "se_mlp_train": (i32, [P, P, P, i64, i32, i32, ctypes.c_float, P, i32]),
+            "se_mlp_save": (i32, [P, ctypes.c_char_p]),
+            "se_mlp_load": (i32, [P, ctypes.c_char_p]),
         }
         for name, (res, args) in sigs.items():
             fn = getattr(L, name)
@@ -144,7 +159,8 @@ class Context:
     """One se_ctx: device memory and a CUDA stream for one host thread."""
 
     def __init__(self, code_bits=63, root_compat=True, build_octree=True, viewpoint=(0.0, 0.0, 0.0),
-                 eigengap_fp64=1e-4, leaf_bucket=32, device=0, stream=None, seed_halo=16):
+                 eigengap_fp64=1e-4, leaf_bucket=32, device=0, stream=None, seed_halo=16, learned=False,
+                 learned_skip_seed=False):
         L = lib()
         o = SeOptions()
         L.se_options_init(ctypes.byref(o))
@@ -158,6 +174,8 @@ class Context:
         o.device = int(device)
         o.stream = stream
         o.seed_halo = int(seed_halo)
+        o.learned = int(bool(learned))
+        o.learned_skip_seed = int(bool(learned_skip_seed))
         self.options = o
         h = ctypes.c_void_p()
         rc = L.se_create(ctypes.byref(h), ctypes.byref(o))
@@ -292,6 +310,69 @@ class Context:
         st = SeStats()
         self._check(lib().se_get_stats(self._h, ctypes.byref(st)), "se_get_stats")
         return {n: getattr(st, n) for n in STAT_NAMES}
+
+    # -- learned search radius ----------------------------------------------
+    def set_learned(self, on, skip_seed=False):
+        """Switch the learned starting bound on or off for later queries."""
+        self._check(lib().se_mlp_enable(self._h, int(bool(on)), int(bool(skip_seed))), "se_mlp_enable")
+
+    def features(self, start=0, count=None):
+        start, count = self._range(start, count)
+        out = np.zeros((count, MLP_FEATURES), np.float32)
+        self._check(lib().se_features(self._h, start, count, _ptr(out)[0], SE_MEM_HOST), "se_features")
+        return out
+
+    def mlp_init(self, seed=0):
+        self._check(lib().se_mlp_init(self._h, seed), "se_mlp_init")
+
+    def mlp_params(self, params=None):
+        if params is None:
+            out = np.zeros(MLP_PARAMS, np.float32)
+            self._check(lib().se_mlp_params(self._h, _ptr(out)[0], 0, SE_MEM_HOST), "se_mlp_params")
+            return out
+        p = np.ascontiguousarray(params, np.float32)
+        assert p.size == MLP_PARAMS
+        self._check(lib().se_mlp_params(self._h, _ptr(p)[0], 1, SE_MEM_HOST), "se_mlp_params")
+
+    def mlp_set_margin(self, margin):
+        self._check(lib().se_mlp_set_margin(self._h, float(margin)), "se_mlp_set_margin")
+
+    def mlp_forward(self, X):
+        X = np.ascontiguousarray(X, np.float32)
+        out = np.zeros(X.shape[0], np.float32)
+        self._check(lib().se_mlp_forward(self._h, _ptr(X)[0], X.shape[0], _ptr(out)[0], SE_MEM_HOST), "se_mlp_forward")
+        return out
+
+    def mlp_predict(self, start=0, count=None):
+        start, count = self._range(start, count)
+        y = np.zeros(count, np.float32)
+        r2 = np.zeros(count, np.float32)
+        self._check(lib().se_mlp_predict(self._h, start, count, _ptr(y)[0], _ptr(r2)[0], SE_MEM_HOST),
+                    "se_mlp_predict")
+        return y, r2
+
+    def mlp_grad(self, X, y):
+        X = np.ascontiguousarray(X, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        g = np.zeros(MLP_PARAMS, np.float32)
+        loss = np.zeros(1, np.float32)
+        self._check(lib().se_mlp_grad(self._h, _ptr(X)[0], _ptr(y)[0], X.shape[0], _ptr(g)[0], _ptr(loss)[0],
+                                      SE_MEM_HOST), "se_mlp_grad")
+        return float(loss[0]), g
+
+    def mlp_train(self, X, y, steps, batch, lr):
+        X = np.ascontiguousarray(X, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        losses = np.zeros(max(steps, 1), np.float32)
+        self._check(lib().se_mlp_train(self._h, _ptr(X)[0], _ptr(y)[0], X.shape[0], steps, batch, float(lr),
+                                       _ptr(losses)[0], SE_MEM_HOST), "se_mlp_train")
+        return losses[:steps]
+
+    def mlp_save(self, path):
+        self._check(lib().se_mlp_save(self._h, str(path).encode()), "se_mlp_save")
+
+    def mlp_load(self, path):
+        self._check(lib().se_mlp_load(self._h, str(path).encode()), "se_mlp_load")
 
     def profile(self):
         p = SeProfile()

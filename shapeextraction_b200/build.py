@@ -20,7 +20,7 @@ CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 BUILD_DIR = os.path.join(ROOT, "_build")
 LIB = os.path.join(PKG, "libshapex.so")
-SOURCES = ["capi.cu", "build.cu", "knn.cu", "static_sort.cu"]
+SOURCES = ["capi.cu", "build.cu", "knn.cu", "mlp.cu", "static_sort.cu"]
 HEADERS = ["common.cuh", "pipeline.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

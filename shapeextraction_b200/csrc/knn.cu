@@ -123,10 +123,12 @@ struct QArgs {
     int code_bits;
     int bucket;
     int seed_halo;
+    const float* learned_r2;
+    int learned_skip_seed;
 };
 
 struct Counters {
-    int cand = 0, ins = 0, merge = 0, buckets = 0;
+    int cand = 0, ins = 0, merge = 0, buckets = 0, lmiss = 0;
 };
 
 // Merge every lane's buffered candidates into its list; the warp steps
@@ -399,124 +401,149 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn(const float4* __restrict__ 
 
     TopK<K, EXACT> tk;
     tk.init(a.k);
-    int bc = 0;  // buffered candidates of this lane
     Counters ct;
-
-    // Seed: each lane walks the Morton window outwards from its own position
-    // (0, +1, -1, +2, ...), so its first candidates are its index neighbours.
-    for (int i = lane; i < S; i += 32) W.pts[i] = __ldg(pts + w0 + i);
-    __syncwarp();
-    {
-        const int p = EXT ? (int)(center + 16 - w0) : (int)(center + lane - w0);
-        const int reach = max(p, S - 1 - p);
-        const int steps = 2 * (int)__reduce_max_sync(FULL, (unsigned)(active ? reach : 0)) + 1;
-        // the first K spiral candidates fill the list directly, then one sort
+    uint32_t steps = 0;
+    // With a learned radius, attempt 0 searches with the predicted bound as a
+    // cap; a lane whose k-th neighbour lies beyond its cap (the cap pruned
+    // points that could belong to its k best) is searched again without it.
+    const bool learned = a.learned_r2 != nullptr;
+    const float cap0 = (learned && active) ? __ldg(a.learned_r2 + qo) : INFINITY;
+    bool act = active;
+    for (int attempt = learned ? 0 : 1; attempt < 2; ++attempt) {
+        const float cap = attempt == 0 ? cap0 : INFINITY;
+        const bool seed = attempt == 1 || !a.learned_skip_seed;
+        const int64_t sw0 = seed ? w0 : 0, sw1 = seed ? w1 : 0;  // points offered by the seed
+        if (act) tk.init(a.k);
+        int bc = 0;  // buffered candidates of this lane
+        if (seed) {
+            // Seed: each lane walks the Morton window outwards from its own
+            // position (0, +1, -1, +2, ...), so its first candidates are its
+            // index neighbours.
+            __syncwarp();
+            for (int i = lane; i < S; i += 32) W.pts[i] = __ldg(pts + w0 + i);
+            __syncwarp();
+            const int p = EXT ? (int)(center + 16 - w0) : (int)(center + lane - w0);
+            const int reach = max(p, S - 1 - p);
+            const int nsteps = 2 * (int)__reduce_max_sync(FULL, (unsigned)(act ? reach : 0)) + 1;
+            // the first K spiral candidates fill the list directly, then one sort
+            if (act) {
 #pragma unroll
-        for (int t = 0; t < K; ++t) {
-            const int off = (t & 1) ? (t + 1) >> 1 : -(t >> 1);
-            const int iw = p + off;
-            unsigned long long kv = kEmptyKey;
-            if (active && iw >= 0 && iw < S) {
-                const float4 q = W.pts[iw];
-                kv = pack_key(dist2(qx, qy, qz, q.x, q.y, q.z), w0 + iw);
+                for (int t = 0; t < K; ++t) {
+                    const int off = (t & 1) ? (t + 1) >> 1 : -(t >> 1);
+                    const int iw = p + off;
+                    unsigned long long kv = kEmptyKey;
+                    if (iw >= 0 && iw < S) {
+                        const float4 q = W.pts[iw];
+                        kv = pack_key(dist2(qx, qy, qz, q.x, q.y, q.z), w0 + iw);
+                    }
+                    tk.key[t] = kv;
+                }
+                tk.sort_filled();
             }
-            tk.key[t] = kv;
+            float tau = fminf(tk.tau(), cap);
+            for (int t = K; t < nsteps; ++t) {
+                const int off = (t & 1) ? (t + 1) >> 1 : -(t >> 1);
+                const int iw = p + off;
+                if (act && iw >= 0 && iw < S) {
+                    const float4 q = W.pts[iw];
+                    if (dist2(qx, qy, qz, q.x, q.y, q.z) <= tau) W.buf[bc++][lane] = (int32_t)(w0 + iw);
+                }
+                if (__any_sync(FULL, bc == kBuf)) {
+                    flush(tk, bc, W, lane, ct, pts, qx, qy, qz);
+                    tau = fminf(tk.tau(), cap);
+                }
+            }
+            flush(tk, bc, W, lane, ct, pts, qx, qy, qz);
         }
-        tk.sort_filled();
-        float tau = tk.tau();
-        for (int t = K; t < steps; ++t) {
-            const int off = (t & 1) ? (t + 1) >> 1 : -(t >> 1);
-            const int iw = p + off;
-            if (active && iw >= 0 && iw < S) {
-                const float4 q = W.pts[iw];
-                if (dist2(qx, qy, qz, q.x, q.y, q.z) <= tau) W.buf[bc++][lane] = (int32_t)(w0 + iw);
-            }
-            if (__any_sync(FULL, bc == kBuf)) {
-                flush(tk, bc, W, lane, ct, pts, qx, qy, qz);
-                tau = tk.tau();
+
+        if (u >= 2 && (sw0 > 0 || sw1 < u)) {
+            int sp = 1;
+            if (lane == 0) W.stack[0] = 0;
+            __syncwarp();
+            const uint32_t step_cap = (uint32_t)min64(2 * u + 64, 0x7fffffff);
+            while (sp > 0) {
+                --sp;
+                const int32_t node = W.stack[sp];
+                __syncwarp();
+                if (++steps > step_cap || node < 0 || node >= u - 1) {
+                    if (lane == 0) set_err(&st->err, steps > step_cap ? ERRBIT_SEARCH_LIMIT : ERRBIT_BOUNDS);
+                    break;
+                }
+                const SNode* sn = snodes + node;
+                const float4 lo_l = __ldg(&sn->lo_l), hi_l = __ldg(&sn->hi_l);
+                const float4 lo_r = __ldg(&sn->lo_r), hi_r = __ldg(&sn->hi_r);
+                const int32_t refl = __float_as_int(lo_l.w), refr = __float_as_int(lo_r.w);
+                const int32_t cntl = __float_as_int(hi_l.w), cntr = __float_as_int(hi_r.w);
+                const uint32_t u32 = (uint32_t)u;
+                const bool okl = cntl <= a.bucket ? (cntl >= 1 && (uint32_t)refl <= u32 - (uint32_t)cntl)
+                                                  : (uint32_t)refl < u32 - 1;
+                const bool okr = cntr <= a.bucket ? (cntr >= 1 && (uint32_t)refr <= u32 - (uint32_t)cntr)
+                                                  : (uint32_t)refr < u32 - 1;
+                if (!(okl && okr)) {
+                    if (lane == 0) set_err(&st->err, ERRBIT_BOUNDS);
+                    break;
+                }
+                const float tau = fminf(tk.tau(), cap);
+                const float dl = box_dist2(qx, qy, qz, lo_l.x, lo_l.y, lo_l.z, hi_l.x, hi_l.y, hi_l.z);
+                const float dr = box_dist2(qx, qy, qz, lo_r.x, lo_r.y, lo_r.z, hi_r.x, hi_r.y, hi_r.z);
+                const uint32_t bl = __ballot_sync(FULL, act && dl <= tau);
+                const uint32_t br = __ballot_sync(FULL, act && dr <= tau);
+                if (!(bl | br)) continue;
+                const uint32_t vote = __ballot_sync(FULL, act && dl <= dr);
+                const int nact = __popc(__ballot_sync(FULL, act));
+                const bool leftFirst = 2 * __popc(vote) >= nact;
+#pragma unroll
+                for (int o = 0; o < 2; ++o) {
+                    const bool left = (o == 0) == leftFirst;
+                    const int32_t cnt = left ? cntl : cntr;
+                    if (cnt > a.bucket) continue;
+                    const int32_t first = left ? refl : refr;
+                    if (first >= sw0 && first + cnt <= sw1) continue;  // all of it was in the seed window
+                    const float bnd = fminf(tk.tau(), cap);
+                    const bool need = act && (left ? dl : dr) <= bnd;
+                    const uint32_t needm = __ballot_sync(FULL, need);
+                    if (!needm) continue;
+                    if (__any_sync(FULL, bc + cnt > kBuf)) flush(tk, bc, W, lane, ct, pts, qx, qy, qz);
+                    ++ct.buckets;
+                    const float b2 = fminf(tk.tau(), cap);
+                    if (3 * __popc(needm) < 2 * cnt)
+                        scan_sparse(first, cnt, needm, qx, qy, qz, b2, bc, W, pts, (int32_t)sw0, (int32_t)sw1, lane);
+                    else
+                        scan_chunk(first, cnt, need, qx, qy, qz, b2, bc, W, pts, (int32_t)sw0, (int32_t)sw1, lane);
+                }
+#pragma unroll
+                for (int o = 1; o >= 0; --o) {
+                    const bool left = (o == 0) == leftFirst;
+                    if ((left ? cntl : cntr) <= a.bucket || !(left ? bl : br)) continue;
+                    if (sp >= kStackDepth) {
+                        if (lane == 0) set_err(&st->err, ERRBIT_STACK);
+                        continue;
+                    }
+                    if (lane == 0) W.stack[sp] = left ? refl : refr;
+                    ++sp;
+                }
+                __syncwarp();
             }
         }
         flush(tk, bc, W, lane, ct, pts, qx, qy, qz);
-    }
-
-    uint32_t steps = 0;
-    if (u >= 2 && (w0 > 0 || w1 < u)) {
-        int sp = 1;
-        if (lane == 0) W.stack[0] = 0;
-        __syncwarp();
-        const uint32_t cap = (uint32_t)min64(u + 64, 0x7fffffff);
-        while (sp > 0) {
-            --sp;
-            const int32_t node = W.stack[sp];
-            __syncwarp();
-            if (++steps > cap || node < 0 || node >= u - 1) {
-                if (lane == 0) set_err(&st->err, steps > cap ? ERRBIT_SEARCH_LIMIT : ERRBIT_BOUNDS);
-                break;
-            }
-            const SNode* sn = snodes + node;
-            const float4 lo_l = __ldg(&sn->lo_l), hi_l = __ldg(&sn->hi_l);
-            const float4 lo_r = __ldg(&sn->lo_r), hi_r = __ldg(&sn->hi_r);
-            const int32_t refl = __float_as_int(lo_l.w), refr = __float_as_int(lo_r.w);
-            const int32_t cntl = __float_as_int(hi_l.w), cntr = __float_as_int(hi_r.w);
-            const uint32_t u32 = (uint32_t)u;
-            const bool okl = cntl <= a.bucket ? (cntl >= 1 && (uint32_t)refl <= u32 - (uint32_t)cntl)
-                                              : (uint32_t)refl < u32 - 1;
-            const bool okr = cntr <= a.bucket ? (cntr >= 1 && (uint32_t)refr <= u32 - (uint32_t)cntr)
-                                              : (uint32_t)refr < u32 - 1;
-            if (!(okl && okr)) {
-                if (lane == 0) set_err(&st->err, ERRBIT_BOUNDS);
-                break;
-            }
-            const float tau = tk.tau();
-            const float dl = box_dist2(qx, qy, qz, lo_l.x, lo_l.y, lo_l.z, hi_l.x, hi_l.y, hi_l.z);
-            const float dr = box_dist2(qx, qy, qz, lo_r.x, lo_r.y, lo_r.z, hi_r.x, hi_r.y, hi_r.z);
-            const uint32_t bl = __ballot_sync(FULL, active && dl <= tau);
-            const uint32_t br = __ballot_sync(FULL, active && dr <= tau);
-            if (!(bl | br)) continue;
-            const uint32_t vote = __ballot_sync(FULL, active && dl <= dr);
-            const int nact = __popc(__ballot_sync(FULL, active));
-            const bool leftFirst = 2 * __popc(vote) >= nact;
-#pragma unroll
-            for (int o = 0; o < 2; ++o) {
-                const bool left = (o == 0) == leftFirst;
-                const int32_t cnt = left ? cntl : cntr;
-                if (cnt > a.bucket) continue;
-                const int32_t first = left ? refl : refr;
-                if (first >= w0 && first + cnt <= w1) continue;  // all of it was in the seed window
-                const bool need = active && (left ? dl : dr) <= tk.tau();
-                const uint32_t needm = __ballot_sync(FULL, need);
-                if (!needm) continue;
-                if (__any_sync(FULL, bc + cnt > kBuf)) flush(tk, bc, W, lane, ct, pts, qx, qy, qz);
-                ++ct.buckets;
-                if (3 * __popc(needm) < 2 * cnt)
-                    scan_sparse(first, cnt, needm, qx, qy, qz, tk.tau(), bc, W, pts, (int32_t)w0, (int32_t)w1, lane);
-                else
-                    scan_chunk(first, cnt, need, qx, qy, qz, tk.tau(), bc, W, pts, (int32_t)w0, (int32_t)w1, lane);
-            }
-#pragma unroll
-            for (int o = 1; o >= 0; --o) {
-                const bool left = (o == 0) == leftFirst;
-                if ((left ? cntl : cntr) <= a.bucket || !(left ? bl : br)) continue;
-                if (sp >= kStackDepth) {
-                    if (lane == 0) set_err(&st->err, ERRBIT_STACK);
-                    continue;
-                }
-                if (lane == 0) W.stack[sp] = left ? refl : refr;
-                ++sp;
-            }
-            __syncwarp();
+        if (attempt == 0) {
+            const bool miss = act && !(tk.tau() <= cap);
+            ct.lmiss += miss;
+            act = miss;
+            if (!__any_sync(FULL, act)) break;
         }
     }
-    flush(tk, bc, W, lane, ct, pts, qx, qy, qz);
     {
         const unsigned cand = __reduce_add_sync(FULL, (unsigned)ct.cand);
         const unsigned ins = __reduce_add_sync(FULL, (unsigned)ct.ins);
+        const unsigned lmiss = __reduce_add_sync(FULL, (unsigned)ct.lmiss);
         if (lane == 0) {
             atomicAdd(&st->counters[CNT_NODES], (unsigned long long)steps);
             atomicAdd(&st->counters[CNT_BUCKETS], (unsigned long long)ct.buckets);
             atomicAdd(&st->counters[CNT_MERGE], (unsigned long long)ct.merge);
             atomicAdd(&st->counters[CNT_CANDIDATES], (unsigned long long)cand);
             atomicAdd(&st->counters[CNT_INSERTS], (unsigned long long)ins);
+            if (lmiss) atomicAdd(&st->counters[CNT_LEARNED_MISS], (unsigned long long)lmiss);
         }
     }
     if (!active) return;
@@ -583,6 +610,8 @@ cudaError_t enqueue_query(const BuildBufs& b, const QueryParams& q, cudaStream_t
     a.code_bits = q.code_bits;
     a.bucket = q.bucket;
     a.seed_halo = q.seed_halo;
+    a.learned_r2 = q.learned_r2;
+    a.learned_skip_seed = q.learned_skip_seed;
     if (a.seed_halo > kMaxHalo) a.seed_halo = kMaxHalo;
     if (a.seed_halo < 0) a.seed_halo = 0;
     const bool ext = q.ext_queries != nullptr;

@@ -21,7 +21,8 @@ constexpr int kScanTile = kScanThreads * kScanIpt;
 
 // Query counters: fp64 solves, nodes visited, buckets scanned, candidates,
 // merge steps, inserts.
-enum { CNT_FP64 = 0, CNT_NODES, CNT_BUCKETS, CNT_CANDIDATES, CNT_MERGE, CNT_INSERTS, kQueryCounters };
+enum { CNT_FP64 = 0, CNT_NODES, CNT_BUCKETS, CNT_CANDIDATES, CNT_MERGE, CNT_INSERTS, CNT_LEARNED_MISS,
+       kQueryCounters };
 
 // Small device-resident state of one build (zeroed at the start of each build).
 struct DevState {
@@ -120,6 +121,41 @@ cudaError_t enqueue_build(const BuildBufs& b, const BuildParams& p, cudaStream_t
 // Enqueue only the octree stage (used to redo it after a capacity regrow).
 cudaError_t enqueue_octree(const BuildBufs& b, const BuildParams& p, cudaStream_t s, int num_sms, int* launches);
 
+// ---- learned search-radius proposal (mlp.cu) --------------------------------
+constexpr int kMlpF = 32;  // features per point
+constexpr int kMlpH = 64;  // hidden width
+// FP32 master parameters, one flat array.
+struct MlpLayout {
+    static constexpr int W1 = 0;                   // [kMlpF][kMlpH], input-major
+    static constexpr int B1 = W1 + kMlpF * kMlpH;  // [kMlpH]
+    static constexpr int W2 = B1 + kMlpH;          // [kMlpH][kMlpH], input-major
+    static constexpr int B2 = W2 + kMlpH * kMlpH;  // [kMlpH]
+    static constexpr int W3 = B2 + kMlpH;          // [kMlpH]
+    static constexpr int B3 = W3 + kMlpH;          // scalar
+    static constexpr int N = B3 + 1;
+};
+constexpr int kMlpParams = MlpLayout::N;
+
+// Training work arrays for n samples.
+struct MlpWork {
+    float* yhat;  // n
+    float* h1;    // n x kMlpH
+    float* h2;    // n x kMlpH
+    float* dy;    // n
+    float* dh1;   // n x kMlpH
+    float* dh2;   // n x kMlpH
+};
+
+cudaError_t enqueue_features(const BuildBufs& b, int64_t u, int code_bits, int64_t start, int64_t count, float* out,
+                             cudaStream_t s);
+cudaError_t enqueue_predict_radius(const BuildBufs& b, const float* params, float margin, int64_t u, int code_bits,
+                                   int64_t start, int64_t count, float* r2_out, float* yhat_out, cudaStream_t s);
+cudaError_t enqueue_mlp_forward(const float* params, const float* X, int64_t n, float* yhat, float* h1, float* h2,
+                                cudaStream_t s);
+cudaError_t enqueue_mlp_grad(const float* params, const float* X, const float* y, int64_t n, MlpWork& w, float* grads,
+                             float* loss, cudaStream_t s);
+cudaError_t enqueue_adam(float* params, const float* grads, float* m, float* v, float lr, int step, cudaStream_t s);
+
 // Sort n 64-bit keys in place in `keys` (ascending) with the onesweep passes;
 // `tmp` (n keys), `lookback` (256 words per 4096-key tile) and `st` are scratch.
 cudaError_t enqueue_sort_keys(uint64_t* keys, uint64_t* tmp, int64_t n, uint32_t* lookback, DevState* st,
@@ -139,6 +175,8 @@ struct QueryParams {
     int code_bits;
     int bucket;
     int seed_halo;
+    const float* learned_r2;  // per query: starting bound from the learned radius, or nullptr
+    int learned_skip_seed;    // with learned_r2: skip the Morton-window seed
 };
 
 cudaError_t enqueue_query(const BuildBufs& b, const QueryParams& q, cudaStream_t s, int num_sms);

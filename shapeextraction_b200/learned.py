@@ -1,0 +1,57 @@
+"""Learned search-radius proposal: training and use.
+
+The model (a 32 -> 64 -> 64 -> 1 MLP, BF16 weights and activations, FP32
+accumulation) predicts y = log2(r_k^2 / range^2) for every tree point from
+occupancy features of the built tree, where r_k is the distance to the point's
+k-th neighbour and range the cloud's extent. Training targets are the exact
+k-th-neighbour distances of the plain search on a held-out cloud; training runs
+on the GPU through the C ABI (se_mlp_train: the library's forward, backward and
+Adam kernels). A log-margin, set from a high quantile of the training
+residuals, turns predictions into upper bounds; the search starts from that
+bound and re-searches, without it, any query it underestimates, so kNN stays
+exact whatever the model predicts.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from ._native import Context
+
+B3 = 6336  # index of the output bias in the flat parameter vector
+
+
+def radius_targets(ctx: Context, k: int) -> np.ndarray:
+    """log2(r_k^2 / range^2) of every tree point, from the exact search."""
+    info = ctx.info()
+    rng = float(info["max_coord"]) - float(info["min_coord"])
+    _, d2 = ctx.knn_self(k, with_d2=True)
+    r2 = np.maximum(d2[:, k - 1].astype(np.float64), 1e-30)
+    return (np.log2(r2) - 2.0 * np.log2(rng)).astype(np.float32)
+
+
+def train_radius_model(ctx: Context, k: int, steps: int = 1500, batch: int = 8192, lr: float = 2e-3, seed: int = 0,
+                       quantile: float = 0.99, max_rows: int = 1_000_000) -> dict:
+    """Train the context's model on its own built cloud (the held-out cloud)
+    and calibrate the margin. Returns the losses and the calibration."""
+    X = ctx.features()
+    y = radius_targets(ctx, k)
+    rng = np.random.default_rng(seed)
+    perm = rng.permutation(y.size)[:max_rows]
+    Xs, ys = np.ascontiguousarray(X[perm]), np.ascontiguousarray(y[perm])
+    ctx.mlp_init(seed)
+    p = ctx.mlp_params()
+    p[B3] = float(ys.mean())
+    ctx.mlp_params(p)
+    losses = ctx.mlp_train(Xs, ys, steps, batch, lr)
+    yhat, _ = ctx.mlp_predict()  # tensor-core path, the one queries use
+    res = y.astype(np.float64) - yhat
+    margin = float(np.quantile(res, quantile))
+    ctx.mlp_set_margin(margin)
+    return {"losses": losses, "margin": margin, "quantile": quantile, "rows": int(ys.size),
+            "residual_std": float(res.std()), "target_mean": float(y.mean())}
+
+
+def transfer(src: Context, dst: Context, margin: float) -> None:
+    """Copy a trained model (parameters and margin) into another context."""
+    dst.mlp_params(src.mlp_params())
+    dst.mlp_set_margin(margin)
