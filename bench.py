@@ -177,31 +177,57 @@ def run_ours(a):
         torch.cuda.synchronize()
         return sum(s.elapsed_time(e) for s, e in ev)
 
-    for _ in range(a.warmup):
-        step_device()
-        step_e2e()
-    torch.cuda.synchronize()
+    def measure():
+        for _ in range(a.warmup):
+            step_device()
+            step_e2e()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        clk = Clocks(local)
+        clk.start()
+        profs = []
+        ms_dev = timed(step_device, a.steps, profs)
+        stats = ctx.stats()
+        ms_e2e = timed(step_e2e, a.steps)
+        clocks = clk.stop()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+            t = torch.tensor([ms_dev, ms_e2e], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms_dev, ms_e2e = float(t[0]), float(t[1])
+        return {"ms_dev": ms_dev, "ms_e2e": ms_e2e, "profs": profs, "stats": stats, "clocks": clocks}
+
     if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    clk = Clocks(local)
-    clk.start()
-    profs = []
-    ms_dev = timed(step_device, a.steps, profs)
-    stats = ctx.stats()
-    ms_e2e = timed(step_e2e, a.steps)
-    clocks = clk.stop()
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-        t = torch.tensor([ms_dev, ms_e2e], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_dev, ms_e2e = float(t[0]), float(t[1])
         tu = torch.tensor([u], dtype=torch.int64, device="cuda")
         dist.all_reduce(tu, op=dist.ReduceOp.SUM)
         u_all = int(tu[0])
     else:
         u_all = u
+
+    plain = measure()
+    lrn = None
+    if not a.no_learned:
+        from shapeextraction_b200 import learned
+
+        # train on a held-out cloud of the same generator and size (another seed)
+        xt, yt, zt = wl["gen"](101 + rank)
+        t0 = time.perf_counter()
+        ctx.build(xt, yt, zt)
+        rep = learned.train_radius_model(ctx, k, steps=a.train_steps, batch=8192, lr=2e-3, seed=rank)
+        train_s = time.perf_counter() - t0
+        ctx.build(dx, dy, dz)
+        ctx.set_learned(True, skip_seed=not a.learned_keep_seed)
+        lrn = measure()
+        ctx.set_learned(False)
+        lrn["train"] = {"seconds_incl_features_and_targets": train_s, "steps": a.train_steps,
+                        "final_loss": float(rep["losses"][-20:].mean()), "first_loss": float(rep["losses"][:20].mean()),
+                        "margin_log2": rep["margin"], "residual_std": rep["residual_std"],
+                        "held_out_seed": 101 + rank}
+    head = lrn if lrn is not None else plain
+    ms_dev, ms_e2e, profs, stats, clocks = head["ms_dev"], head["ms_e2e"], head["profs"], head["stats"], head["clocks"]
 
     # dominant kernel: the fused kNN + normals kernel
     q_ms = statistics.mean(p["query_ms"] for p in profs)
@@ -243,6 +269,18 @@ def run_ours(a):
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": peak_kind, "traffic": traffic, "alg_bytes_per_launch": int(alg_bytes),
                          "launch_ms": q_ms},
+            "pipeline": "learned-radius" if lrn is not None else "plain",
+            "plain": {"value": u_all * a.steps / (plain["ms_dev"] * 1e-3), "ms_per_step": plain["ms_dev"] / a.steps,
+                      "e2e_value": u_all * a.steps / (plain["ms_e2e"] * 1e-3),
+                      "knn_normals_ms": statistics.mean(p["query_ms"] for p in plain["profs"]),
+                      "search_per_query": {key: plain["stats"][key] / max(u, 1) for key in
+                                           ("candidates", "inserts")}},
+            "learned": None if lrn is None else {
+                "value": u_all * a.steps / (lrn["ms_dev"] * 1e-3), "ms_per_step": lrn["ms_dev"] / a.steps,
+                "e2e_value": u_all * a.steps / (lrn["ms_e2e"] * 1e-3),
+                "knn_normals_ms": statistics.mean(p["query_ms"] for p in lrn["profs"]),
+                "misses_per_query": lrn["stats"]["learned_misses"] / max(u, 1),
+                "skip_seed": not a.learned_keep_seed, **lrn["train"]},
             "stages_ms": {**build_ms, "knn_normals": q_ms},
             "gpu_launches": int(launches),
             "fp64_solves_last_step": stats["fp64_solves"],
@@ -375,6 +413,10 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=200_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-cuda", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="time only the plain search")
+    ap.add_argument("--learned-keep-seed", action="store_true",
+                    help="with the learned radius, still offer the Morton-window seed")
+    ap.add_argument("--train-steps", type=int, default=1500)
     a = ap.parse_args()
     if a.warmup < 3:
         a.warmup = 3
