@@ -151,6 +151,19 @@ int se_knn(se_ctx* ctx, int k, const float* queries_xyz, int64_t n_queries, int3
  * kernel. out_xyz: count normals, AoS xyz (std::vector<Point> layout). */
 int se_normals(se_ctx* ctx, int k, int64_t start, int64_t count, float* out_xyz, int mem);
 
+/* Batched normal estimation over n_clouds independent clouds; no counterpart
+ * in the reference (one cloud per call there). The clouds are concatenated
+ * SoA: cloud c is points [offsets[c], offsets[c+1]) of x, y, z, with its own
+ * k = ks[c] (1..32). Every cloud runs the whole path (bbox, codes, sort,
+ * dedup, radix tree, search hierarchy, exact kNN, normals; no octree) with
+ * device-side sizes, spread largest-first over the context's internal streams
+ * with no host synchronisation between clouds. out_normals holds
+ * offsets[n_clouds] rows of xyz: cloud c's u_c normals (its unique points in
+ * Morton order) start at row offsets[c]; out_u[c] = u_c. offsets, ks and out_u
+ * are host arrays; x, y, z and out_normals follow `mem`. */
+int se_normals_batch(se_ctx* ctx, const float* x, const float* y, const float* z, const int64_t* offsets,
+                     int n_clouds, const int32_t* ks, float* out_normals, int64_t* out_u, int mem);
+
 /* Work counters of the last se_normals/se_knn/se_knn_self call (diagnostics). */
 typedef struct se_stats {
     int64_t fp64_solves;     /* queries whose eigensolve took the FP64 path */

@@ -30,7 +30,7 @@ EXPORTS = [
     "se_build", "se_get_info", "se_get_device_views", "se_get_codes", "se_get_radix", "se_get_octree",
     "se_get_points", "se_knn_self", "se_knn", "se_normals", "se_get_stats", "se_get_profile", "se_synchronize",
     "se_sort_keys_static", "se_features", "se_mlp_init", "se_mlp_params", "se_mlp_enable", "se_mlp_set_margin", "se_mlp_forward",
-    "se_mlp_predict", "se_mlp_grad", "se_mlp_train", "se_mlp_save", "se_mlp_load",
+    "se_mlp_predict", "se_mlp_grad", "se_mlp_train", "se_mlp_save", "se_mlp_load", "se_normals_batch",
 ]
 MLP_FEATURES = 32
 MLP_PARAMS = 6337
@@ -129,6 +129,7 @@ def lib():
             "se_mlp_train": (i32, [P, P, P, i64, i32, i32, ctypes.c_float, P, i32]),
             "se_mlp_save": (i32, [P, ctypes.c_char_p]),
             "se_mlp_load": (i32, [P, ctypes.c_char_p]),
+            "se_normals_batch": (i32, [P, P, P, P, P, i32, P, P, P, i32]),
         }
         for name, (res, args) in sigs.items():
             fn = getattr(L, name)
@@ -373,6 +374,35 @@ class Context:
 
     def mlp_load(self, path):
         self._check(lib().se_mlp_load(self._h, str(path).encode()), "se_mlp_load")
+
+    def normals_batch(self, clouds, ks, out=None):
+        """Normals of many independent clouds in one call. `clouds` is a list
+        of (x, y, z) arrays, or one (x, y, z) triple of concatenated torch
+        tensors together with `offsets` given as ks=(ks, offsets). Returns
+        (normals, offsets, u): cloud c's u[c] normals start at row offsets[c]."""
+        if isinstance(ks, tuple):
+            ks, offsets = ks
+            x, y, z = clouds
+            offsets = np.ascontiguousarray(offsets, np.int64)
+        else:
+            sizes = [len(cl[0]) for cl in clouds]
+            offsets = np.zeros(len(clouds) + 1, np.int64)
+            offsets[1:] = np.cumsum(sizes)
+            x, y, z = (np.ascontiguousarray(np.concatenate([cl[i] for cl in clouds]), np.float32) for i in range(3))
+        ks = np.ascontiguousarray(ks, np.int32)
+        n_clouds = ks.size
+        total = int(offsets[-1])
+        if out is None:
+            if _is_torch(x):
+                import torch
+                out = torch.zeros((total, 3), dtype=torch.float32, device=x.device)
+            else:
+                out = np.zeros((total, 3), np.float32)
+        u = np.zeros(n_clouds, np.int64)
+        px, mem = _ptr(x)
+        self._check(lib().se_normals_batch(self._h, px, _ptr(y)[0], _ptr(z)[0], _ptr(offsets)[0], n_clouds,
+                                           _ptr(ks)[0], _ptr(out)[0], _ptr(u)[0], mem), "se_normals_batch")
+        return out, offsets, u
 
     def profile(self):
         p = SeProfile()

@@ -2,14 +2,26 @@
 // Declarations and the reference interface each entry point replaces are in
 // include/shapex.h.
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <numeric>
 #include <string>
+#include <vector>
 
 #include "pipeline.cuh"
 #include "shapex.h"
 
 using namespace shapex;
+
+// One independent pipeline of the batched path: its own stream, buffers and
+// device state, so that clouds on different lanes overlap on the GPU.
+struct BatchLane {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    BuildBufs b{};
+    int64_t cap = 0;
+};
 
 struct se_ctx {
     se_options opt;
@@ -50,6 +62,18 @@ struct se_ctx {
     int64_t r2_cap = 0;
     float* xs_buf = nullptr;  // staging of host features / targets / outputs
     int64_t xs_cap = 0;
+
+    // batched path
+    std::vector<BatchLane> lanes;
+    cudaEvent_t batch_in_ready = nullptr;
+    float* batch_in = nullptr;   // staged host coordinates (3 x total)
+    float* batch_out = nullptr;  // staged normals for host output
+    int64_t batch_cap = 0;
+    unsigned long long* batch_u = nullptr;  // u per cloud
+    uint32_t* batch_err = nullptr;          // error word per cloud
+    unsigned long long* h_batch_u = nullptr;
+    uint32_t* h_batch_err = nullptr;
+    int batch_clouds_cap = 0;
 
     cudaEvent_t build_ev[kBuildEvents] = {};
     cudaEvent_t query_ev[2] = {};
@@ -381,6 +405,23 @@ int se_destroy(se_ctx* c) {
                          c->mw.yhat, c->mw.h1, c->mw.h2, c->mw.dy, c->mw.dh1, c->mw.dh2};
     for (float* p : mlp_bufs)
         if (p) cudaFree(p);
+    for (BatchLane& l : c->lanes) {
+        if (l.stream) cudaStreamSynchronize(l.stream);
+        void* ptrs[] = {l.b.keys0, l.b.keys1, l.b.lookback, l.b.lookback64, l.b.codes, l.b.pts4, l.b.pts3,
+                        l.b.left_child, l.b.parent, l.b.prefix_n, l.b.has_leaf_left, l.b.has_leaf_right, l.b.sparent,
+                        l.b.leaf_parent, l.b.range_end, l.b.visit, l.b.node_box, l.b.snodes, l.b.st};
+        for (void* p : ptrs)
+            if (p) cudaFree(p);
+        if (l.done) cudaEventDestroy(l.done);
+        if (l.stream) cudaStreamDestroy(l.stream);
+    }
+    if (c->batch_in_ready) cudaEventDestroy(c->batch_in_ready);
+    if (c->batch_in) cudaFree(c->batch_in);
+    if (c->batch_out) cudaFree(c->batch_out);
+    if (c->batch_u) cudaFree(c->batch_u);
+    if (c->batch_err) cudaFree(c->batch_err);
+    if (c->h_batch_u) cudaFreeHost(c->h_batch_u);
+    if (c->h_batch_err) cudaFreeHost(c->h_batch_err);
     for (auto& e : c->build_ev)
         if (e) cudaEventDestroy(e);
     for (auto& e : c->query_ev)
@@ -822,6 +863,175 @@ int se_mlp_load(se_ctx* c, const char* path) {
     if (int rc = se_mlp_params(c, h, 1, SE_MEM_HOST)) return rc;
     c->mlp_margin = margin;
     return SE_OK;
+}
+
+// ---- batched path --------------------------------------------------------------
+
+namespace {
+
+int lane_capacity(se_ctx* c, BatchLane& l, int64_t n) {
+    if (!l.stream) {
+        SE_CUDA(c, cudaStreamCreateWithFlags(&l.stream, cudaStreamNonBlocking), "lane stream");
+        SE_CUDA(c, cudaEventCreateWithFlags(&l.done, cudaEventDisableTiming), "lane event");
+        SE_CUDA(c, cudaMalloc(&l.b.st, sizeof(DevState)), "lane state");
+    }
+    if (n <= l.cap && l.b.keys0) return SE_OK;
+    BuildBufs& b = l.b;
+    const int64_t cap = n < 1024 ? 1024 : n;
+    const int64_t sort_tiles = (cap + kSortTile - 1) / kSortTile;
+    const int64_t scan_tiles = (cap + kScanTile - 1) / kScanTile;
+    SE_CUDA(c, regrow(b.keys0, cap), "alloc lane");
+    SE_CUDA(c, regrow(b.keys1, cap), "alloc lane");
+    SE_CUDA(c, regrow(b.lookback, sort_tiles * 256 + 64), "alloc lane");
+    SE_CUDA(c, regrow(b.lookback64, scan_tiles + 64), "alloc lane");
+    SE_CUDA(c, regrow(b.codes, cap), "alloc lane");
+    SE_CUDA(c, regrow(b.pts4, cap), "alloc lane");
+    SE_CUDA(c, regrow(b.pts3, 3 * cap), "alloc lane");
+    SE_CUDA(c, regrow(b.left_child, cap), "alloc lane");
+    SE_CUDA(c, regrow(b.parent, cap), "alloc lane");
+    SE_CUDA(c, regrow(b.prefix_n, cap), "alloc lane");
+    SE_CUDA(c, regrow(b.has_leaf_left, cap), "alloc lane");
+    SE_CUDA(c, regrow(b.has_leaf_right, cap), "alloc lane");
+    SE_CUDA(c, regrow(b.sparent, cap), "alloc lane");
+    SE_CUDA(c, regrow(b.leaf_parent, cap), "alloc lane");
+    SE_CUDA(c, regrow(b.range_end, cap), "alloc lane");
+    SE_CUDA(c, regrow(b.visit, cap), "alloc lane");
+    SE_CUDA(c, regrow(b.node_box, 2 * cap), "alloc lane");
+    SE_CUDA(c, regrow(b.snodes, cap), "alloc lane");
+    b.cap = cap;
+    l.cap = cap;
+    return SE_OK;
+}
+
+}  // namespace
+
+int se_normals_batch(se_ctx* c, const float* x, const float* y, const float* z, const int64_t* offsets, int n_clouds,
+                     const int32_t* ks, float* out_normals, int64_t* out_u, int mem) {
+    if (int rc = prologue(c)) return rc;
+    if (int rc = check_mem(c, mem)) return rc;
+    if (n_clouds < 0 || (n_clouds > 0 && (!offsets || !ks || !out_u)))
+        return fail(c, SE_ERR_INVALID_ARG, "bad batch description");
+    if (n_clouds == 0) return SE_OK;
+    if (offsets[0] != 0) return fail(c, SE_ERR_INVALID_ARG, "offsets[0] must be 0");
+    for (int i = 0; i < n_clouds; ++i) {
+        if (offsets[i + 1] < offsets[i]) return fail(c, SE_ERR_INVALID_ARG, "offsets must not decrease");
+        if (ks[i] < 1 || ks[i] > 32) return fail(c, SE_ERR_UNSUPPORTED, "k must be in [1, 32]");
+    }
+    const int64_t total = offsets[n_clouds];
+    if (total > ((int64_t)1 << 30)) return fail(c, SE_ERR_INVALID_ARG, "more than 2^30 points in one batch");
+    if (total > 0 && (!x || !y || !z || !out_normals)) return fail(c, SE_ERR_INVALID_ARG, "null pointer");
+    const bool host = mem == SE_MEM_HOST;
+
+    // per-cloud result words and host-input staging
+    if (c->batch_clouds_cap < n_clouds) {
+        if (c->batch_u) cudaFree(c->batch_u);
+        if (c->batch_err) cudaFree(c->batch_err);
+        if (c->h_batch_u) cudaFreeHost(c->h_batch_u);
+        if (c->h_batch_err) cudaFreeHost(c->h_batch_err);
+        c->batch_u = nullptr;
+        c->batch_err = nullptr;
+        c->h_batch_u = nullptr;
+        c->h_batch_err = nullptr;
+        c->batch_clouds_cap = 0;
+        SE_CUDA(c, cudaMalloc(&c->batch_u, sizeof(unsigned long long) * n_clouds), "alloc batch");
+        SE_CUDA(c, cudaMalloc(&c->batch_err, sizeof(uint32_t) * n_clouds), "alloc batch");
+        SE_CUDA(c, cudaMallocHost(&c->h_batch_u, sizeof(unsigned long long) * n_clouds), "alloc batch");
+        SE_CUDA(c, cudaMallocHost(&c->h_batch_err, sizeof(uint32_t) * n_clouds), "alloc batch");
+        c->batch_clouds_cap = n_clouds;
+    }
+    if (!c->batch_in_ready) SE_CUDA(c, cudaEventCreateWithFlags(&c->batch_in_ready, cudaEventDisableTiming), "event");
+    const float *bx = x, *by = y, *bz = z;
+    float* bout = out_normals;
+    if (host && total > 0) {
+        if (c->batch_cap < total) {
+            SE_CUDA(c, regrow(c->batch_in, 3 * total), "alloc batch staging");
+            SE_CUDA(c, regrow(c->batch_out, 3 * total), "alloc batch staging");
+            c->batch_cap = total;
+        }
+        SE_CUDA(c, cudaMemcpyAsync(c->batch_in, x, 4 * total, cudaMemcpyHostToDevice, c->stream), "copy x");
+        SE_CUDA(c, cudaMemcpyAsync(c->batch_in + total, y, 4 * total, cudaMemcpyHostToDevice, c->stream), "copy y");
+        SE_CUDA(c, cudaMemcpyAsync(c->batch_in + 2 * total, z, 4 * total, cudaMemcpyHostToDevice, c->stream),
+                "copy z");
+        bx = c->batch_in;
+        by = c->batch_in + total;
+        bz = c->batch_in + 2 * total;
+        bout = c->batch_out;
+    }
+    SE_CUDA(c, cudaMemsetAsync(c->batch_u, 0, sizeof(unsigned long long) * n_clouds, c->stream), "reset batch");
+    SE_CUDA(c, cudaMemsetAsync(c->batch_err, 0, sizeof(uint32_t) * n_clouds, c->stream), "reset batch");
+    SE_CUDA(c, cudaEventRecord(c->batch_in_ready, c->stream), "event");
+
+    // largest cloud first, each to the lane with the least queued work
+    const int n_lanes = std::min(n_clouds, 8);
+    if ((int)c->lanes.size() < n_lanes) c->lanes.resize(n_lanes);
+    std::vector<int> order(n_clouds);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        return offsets[a + 1] - offsets[a] > offsets[b + 1] - offsets[b];
+    });
+    std::vector<std::vector<int>> queue(n_lanes);
+    std::vector<int64_t> load(n_lanes, 0), need(n_lanes, 0);
+    for (int ci : order) {
+        const int l = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        const int64_t n = offsets[ci + 1] - offsets[ci];
+        queue[l].push_back(ci);
+        load[l] += n + 4096;  // fixed cost per cloud
+        need[l] = std::max(need[l], n);
+    }
+    for (int l = 0; l < n_lanes; ++l) {
+        BatchLane& lane = c->lanes[l];
+        if (int rc = lane_capacity(c, lane, need[l])) return rc;
+        SE_CUDA(c, cudaStreamWaitEvent(lane.stream, c->batch_in_ready, 0), "wait");
+        for (int ci : queue[l]) {
+            const int64_t off = offsets[ci], n = offsets[ci + 1] - offsets[ci];
+            if (n == 0) continue;
+            BuildBufs b = lane.b;
+            b.x = bx + off;
+            b.y = by + off;
+            b.z = bz + off;
+            BuildParams p{n, c->opt.code_bits, 0, 0, c->opt.leaf_bucket};
+            SE_CUDA(c, enqueue_build(b, p, lane.stream, c->num_sms, nullptr, nullptr), "launch batch build");
+            QueryParams q{};
+            q.k = ks[ci];
+            q.start = 0;
+            q.count = n;
+            q.u = n;
+            q.device_count = 1;
+            q.out_normals = bout + 3 * off;
+            q.vx = c->opt.viewpoint[0];
+            q.vy = c->opt.viewpoint[1];
+            q.vz = c->opt.viewpoint[2];
+            q.eigengap_fp64 = c->opt.eigengap_fp64;
+            q.code_bits = c->opt.code_bits;
+            q.bucket = c->opt.leaf_bucket;
+            q.seed_halo = c->opt.seed_halo;
+            SE_CUDA(c, enqueue_query(b, q, lane.stream, c->num_sms), "launch batch query");
+            SE_CUDA(c, cudaMemcpyAsync(c->batch_u + ci, &b.st->u, sizeof(unsigned long long), cudaMemcpyDeviceToDevice,
+                                       lane.stream),
+                    "record u");
+            SE_CUDA(c, cudaMemcpyAsync(c->batch_err + ci, &b.st->err, sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                                       lane.stream),
+                    "record err");
+        }
+        SE_CUDA(c, cudaEventRecord(lane.done, lane.stream), "event");
+        SE_CUDA(c, cudaStreamWaitEvent(c->stream, lane.done, 0), "join");
+    }
+    if (host && total > 0)
+        SE_CUDA(c, cudaMemcpyAsync(out_normals, bout, sizeof(float) * 3 * total, cudaMemcpyDeviceToHost, c->stream),
+                "copy normals");
+    SE_CUDA(c, cudaMemcpyAsync(c->h_batch_u, c->batch_u, sizeof(unsigned long long) * n_clouds,
+                               cudaMemcpyDeviceToHost, c->stream),
+            "read u");
+    SE_CUDA(c, cudaMemcpyAsync(c->h_batch_err, c->batch_err, sizeof(uint32_t) * n_clouds, cudaMemcpyDeviceToHost,
+                               c->stream),
+            "read errors");
+    SE_CUDA(c, cudaStreamSynchronize(c->stream), "synchronize");
+    uint32_t err = 0;
+    for (int i = 0; i < n_clouds; ++i) {
+        out_u[i] = (int64_t)c->h_batch_u[i];
+        err |= c->h_batch_err[i];
+    }
+    return check_err_bits(c, err);
 }
 
 int se_synchronize(se_ctx* c) {

@@ -125,6 +125,7 @@ struct QArgs {
     int seed_halo;
     const float* learned_r2;
     int learned_skip_seed;
+    int device_count;  // 1: u = count = the build's unique-point count, read on the device (start 0)
 };
 
 struct Counters {
@@ -361,11 +362,12 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn(const float4* __restrict__ 
     extern __shared__ __align__(16) unsigned char knn_smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     WarpSmem& W = reinterpret_cast<WarpSmem*>(knn_smem)[warp];
+    const int64_t u = a.device_count ? (int64_t)st->u : a.u;
+    const int64_t count = a.device_count ? u : a.count;
     const int64_t q0 = ((int64_t)blockIdx.x * kKnnWarps + warp) * 32;
-    if (q0 >= a.count) return;  // whole warp
+    if (q0 >= count) return;  // whole warp
     const int64_t qo = q0 + lane;
-    const bool active = qo < a.count;
-    const int64_t u = a.u;
+    const bool active = qo < count;
     float qx, qy, qz;
     int64_t center;  // tree index of the warp's first query (or its code position)
     if (EXT) {
@@ -612,6 +614,7 @@ cudaError_t enqueue_query(const BuildBufs& b, const QueryParams& q, cudaStream_t
     a.seed_halo = q.seed_halo;
     a.learned_r2 = q.learned_r2;
     a.learned_skip_seed = q.learned_skip_seed;
+    a.device_count = q.device_count;
     if (a.seed_halo > kMaxHalo) a.seed_halo = kMaxHalo;
     if (a.seed_halo < 0) a.seed_halo = 0;
     const bool ext = q.ext_queries != nullptr;

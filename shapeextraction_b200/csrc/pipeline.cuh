@@ -177,6 +177,8 @@ struct QueryParams {
     int seed_halo;
     const float* learned_r2;  // per query: starting bound from the learned radius, or nullptr
     int learned_skip_seed;    // with learned_r2: skip the Morton-window seed
+    int device_count;         // 1: query all u points of the build, u read on the device; `count`
+                              // is then an upper bound used only to size the grid
 };
 
 cudaError_t enqueue_query(const BuildBufs& b, const QueryParams& q, cudaStream_t s, int num_sms);
