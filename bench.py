@@ -51,6 +51,9 @@ def _workloads():
                             desc="50M points Gaussian mixture + surfaces, 63-bit codes, k=16"),
         "cube_100k_k10": dict(gen=lambda s: synth.uniform_cube(100_000, s), k=10, code_bits=30,
                               desc="100k uniform points, 30-bit codes, k=10"),
+        "batch_256": dict(gen=lambda s: synth.batched_clouds(256, s), k=None, code_bits=63, batched=True,
+                          desc="256 independent scenes, sizes log-uniform in [1k, 500k], k per cloud in {8,16,32}, "
+                               "one se_normals_batch call"),
     }
 
 
@@ -297,6 +300,108 @@ def run_ours(a):
         dist.destroy_process_group()
 
 
+def run_batch(a):
+    import torch
+    import torch.distributed as dist
+
+    from shapeextraction_b200 import Context, autotune
+
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    wl = _workloads()[a.workload]
+    clouds, ks = wl["gen"](a.seed + rank)
+    ks = np.ascontiguousarray(ks, np.int32)
+    sizes = np.array([len(c[0]) for c in clouds], np.int64)
+    offsets = np.zeros(len(clouds) + 1, np.int64)
+    offsets[1:] = np.cumsum(sizes)
+    total = int(offsets[-1])
+    host = [torch.from_numpy(np.ascontiguousarray(np.concatenate([c[i] for c in clouds]), np.float32)).pin_memory()
+            for i in range(3)]
+    dev = [h.cuda() for h in host]
+    tuning = None
+    if a.autotune:
+        tuning = autotune.tune_batch(clouds, ks, device=local, cache_path=a.autotune_cache)
+        bucket, halo = tuning["leaf_bucket"], tuning["seed_halo"]
+    else:
+        bucket, halo = a.bucket, a.halo
+    stream = torch.cuda.current_stream()
+    ctx = Context(code_bits=wl["code_bits"], device=local, stream=stream.cuda_stream, eigengap_fp64=a.eigengap,
+                  leaf_bucket=bucket, seed_halo=halo)
+    out_dev = torch.empty((total, 3), dtype=torch.float32, device="cuda")
+    out_host = torch.empty((total, 3), dtype=torch.float32).pin_memory()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    _, _, u = ctx.normals_batch(tuple(dev), (ks, offsets), out=out_dev)
+    u_sum = int(u.sum())
+
+    def timed(step, steps):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for i in range(steps):
+            flush.fill_(float(i))
+            ev[i][0].record(stream)
+            step()
+            ev[i][1].record(stream)
+        torch.cuda.synchronize()
+        return sum(s.elapsed_time(e) for s, e in ev)
+
+    step_dev = lambda: ctx.normals_batch(tuple(dev), (ks, offsets), out=out_dev)  # noqa: E731
+    step_e2e = lambda: ctx.normals_batch(tuple(host), (ks, offsets), out=out_host)  # noqa: E731
+    for _ in range(a.warmup):
+        step_dev()
+        step_e2e()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = Clocks(local)
+    clk.start()
+    ms_dev = timed(step_dev, a.steps)
+    ms_e2e = timed(step_e2e, a.steps)
+    clocks = clk.stop()
+    prof = ctx.profile()
+    # per step: the build and query kernels of every cloud, the e2e arm's too
+    launches = 2 * a.steps * (prof["build_launches"] + prof["query_launches"])
+    if world > 1:
+        t = torch.tensor([ms_dev, ms_e2e], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_dev, ms_e2e = float(t[0]), float(t[1])
+        tu = torch.tensor([u_sum], dtype=torch.int64, device="cuda")
+        dist.all_reduce(tu, op=dist.ReduceOp.SUM)
+        u_all = int(tu[0])
+    else:
+        u_all = u_sum
+    # whole-pipeline algorithmic bytes (bbox, encode, sort, dedup, tree, search, normals; no octree)
+    alg = float(np.sum(72 * sizes + (96 + 4 * ks.astype(np.int64)) * u))
+    peak, peak_kind = _peaks()
+    achieved = alg / (ms_dev / a.steps * 1e-3) / 1e9
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cpu = cpu_baseline("scene_2M_k16", a.seed, a.cpu_sample)
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": u_all * a.steps / (ms_dev * 1e-3), "unit": "normals/s", "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_dev / a.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator, no dataset)",
+            "pipeline": "plain (batched)",
+            "config": {"workload": a.workload, "desc": wl["desc"], "clouds": len(clouds), "n_points": total,
+                       "unique_points": u_sum, "k_counts": {str(k): int((ks == k).sum()) for k in (8, 16, 32)},
+                       "leaf_bucket": bucket, "seed_halo": halo, "autotune": tuning,
+                       "l2": "flushed by a 256 MB device write before every timed step",
+                       "parallelism": f"{world} independent replica(s), one batch per GPU"},
+            "e2e": {"value": u_all * a.steps / (ms_e2e * 1e-3), "unit": "normals/s", "ms_per_step": ms_e2e / a.steps,
+                    "h2d_bytes_per_step": 12 * total, "d2h_bytes_per_step": 12 * total},
+            "roofline": {"bound": "hbm", "kernel": "whole batched pipeline (all kernels of one step)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_source": peak_kind, "traffic": None, "alg_bytes_per_launch": alg},
+            "gpu_launches": launches, "clocks": clocks, "cpu_baseline": cpu}), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def cpu_baseline(workload, seed, sample):
     """The reference pipeline restated on the host cores, on a bounded sample."""
     from oracle import oracle as O
@@ -327,6 +432,8 @@ def reference_cuda(workload, seed, reps=3):
     from shapeextraction_b200 import synth
 
     wl = _workloads()[workload]
+    if wl.get("batched"):
+        return {"unavailable": "batched workload: the reference runs one cloud per process call"}
     x, y, z = wl["gen"](seed)
     a = O.build_stages(x, y, z, 63, root_compat=True)["radix"]
     b = O.build_stages(x, y, z, 63, root_compat=False)["radix"]
@@ -359,21 +466,22 @@ def run_reference(a):
     from oracle import oracle as O
     from shapeextraction_b200 import synth
 
+    k_ref = wl["k"] or 16
     if a.workload.startswith("cube"):
         x, y, z = synth.uniform_cube(min(a.cpu_sample, 100_000), a.seed)
     else:
         x, y, z = synth.scene(a.cpu_sample, a.seed)
     for _ in range(a.warmup):
-        O.pipeline_reference(x, y, z, wl["k"])
+        O.pipeline_reference(x, y, z, k_ref)
     times = []
     u = 0
     for _ in range(a.steps):
         t = time.perf_counter()
-        u, _ = O.pipeline_reference(x, y, z, wl["k"])
+        u, _ = O.pipeline_reference(x, y, z, k_ref)
         times.append(time.perf_counter() - t)
     tot = sum(times)
     value = u * a.steps / tot
-    sample = (f"{x.size} points of the same scene generator per step, k={wl['k']}: reference pipeline restated on "
+    sample = (f"{x.size} points of the same scene generator per step, k={k_ref}: reference pipeline restated on "
               "the host (bit-exact build, the reference's approximate octree search, FP32 covariance, FP64 Jacobi)")
     line = {
         "impl": "reference",
@@ -389,7 +497,7 @@ def run_reference(a):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded generator, no dataset)",
-        "config": {"workload": a.workload, "desc": wl["desc"], "k": wl["k"], "code_bits": wl["code_bits"]},
+        "config": {"workload": a.workload, "desc": wl["desc"], "k": k_ref, "code_bits": wl["code_bits"]},
         "cpu_baseline": {"value": value, "unit": "normals/s", "cores": os.cpu_count(), "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": "normals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -417,11 +525,15 @@ def main():
     ap.add_argument("--learned-keep-seed", action="store_true",
                     help="with the learned radius, still offer the Morton-window seed")
     ap.add_argument("--train-steps", type=int, default=1500)
+    ap.add_argument("--autotune", action="store_true", help="pick bucket/halo with the autotuner (cached)")
+    ap.add_argument("--autotune-cache", default=os.path.join(ROOT, "_build", "autotune.json"))
     a = ap.parse_args()
     if a.warmup < 3:
         a.warmup = 3
     if a.impl == "reference":
         run_reference(a)
+    elif _workloads()[a.workload].get("batched"):
+        run_batch(a)
     else:
         run_ours(a)
 

@@ -969,6 +969,7 @@ int se_normals_batch(se_ctx* c, const float* x, const float* y, const float* z, 
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
         return offsets[a + 1] - offsets[a] > offsets[b + 1] - offsets[b];
     });
+    int batch_build_launches = 0, batch_query_launches = 0;
     std::vector<std::vector<int>> queue(n_lanes);
     std::vector<int64_t> load(n_lanes, 0), need(n_lanes, 0);
     for (int ci : order) {
@@ -990,7 +991,10 @@ int se_normals_batch(se_ctx* c, const float* x, const float* y, const float* z, 
             b.y = by + off;
             b.z = bz + off;
             BuildParams p{n, c->opt.code_bits, 0, 0, c->opt.leaf_bucket};
-            SE_CUDA(c, enqueue_build(b, p, lane.stream, c->num_sms, nullptr, nullptr), "launch batch build");
+            int nl = 0;
+            SE_CUDA(c, enqueue_build(b, p, lane.stream, c->num_sms, nullptr, &nl), "launch batch build");
+            batch_build_launches += nl;
+            ++batch_query_launches;
             QueryParams q{};
             q.k = ks[ci];
             q.start = 0;
@@ -1026,6 +1030,8 @@ int se_normals_batch(se_ctx* c, const float* x, const float* y, const float* z, 
                                c->stream),
             "read errors");
     SE_CUDA(c, cudaStreamSynchronize(c->stream), "synchronize");
+    c->build_launches = batch_build_launches;
+    c->query_launches = batch_query_launches;
     uint32_t err = 0;
     for (int i = 0; i < n_clouds; ++i) {
         out_u[i] = (int64_t)c->h_batch_u[i];

@@ -20,32 +20,46 @@ from ._native import Context
 B3 = 6336  # index of the output bias in the flat parameter vector
 
 
-def radius_targets(ctx: Context, k: int) -> np.ndarray:
-    """log2(r_k^2 / range^2) of every tree point, from the exact search."""
+def radius_targets(ctx: Context, k: int, start: int = 0, count: int | None = None) -> np.ndarray:
+    """log2(r_k^2 / range^2) of tree points [start, start+count), from the exact search."""
     info = ctx.info()
     rng = float(info["max_coord"]) - float(info["min_coord"])
-    _, d2 = ctx.knn_self(k, with_d2=True)
+    _, d2 = ctx.knn_self(k, start, count, with_d2=True)
     r2 = np.maximum(d2[:, k - 1].astype(np.float64), 1e-30)
     return (np.log2(r2) - 2.0 * np.log2(rng)).astype(np.float32)
+
+
+def _sample(ctx: Context, k: int, max_rows: int, rng) -> tuple[np.ndarray, np.ndarray]:
+    """Features and targets of all points, or of 64 random Morton-contiguous
+    chunks (spread over the cloud) when it has more than max_rows points."""
+    u = ctx.info()["n_points"]
+    if u <= max_rows:
+        return ctx.features(), radius_targets(ctx, k)
+    chunk = max(1, max_rows // 64)
+    starts = np.sort(rng.choice(u // chunk, size=64, replace=False)) * chunk
+    X = np.concatenate([ctx.features(int(s), chunk) for s in starts])
+    y = np.concatenate([radius_targets(ctx, k, int(s), chunk) for s in starts])
+    return X, y
 
 
 def train_radius_model(ctx: Context, k: int, steps: int = 1500, batch: int = 8192, lr: float = 2e-3, seed: int = 0,
                        quantile: float = 0.99, max_rows: int = 1_000_000) -> dict:
     """Train the context's model on its own built cloud (the held-out cloud)
     and calibrate the margin. Returns the losses and the calibration."""
-    X = ctx.features()
-    y = radius_targets(ctx, k)
     rng = np.random.default_rng(seed)
-    perm = rng.permutation(y.size)[:max_rows]
+    X, y = _sample(ctx, k, max_rows, rng)
+    perm = rng.permutation(y.size)
     Xs, ys = np.ascontiguousarray(X[perm]), np.ascontiguousarray(y[perm])
     ctx.mlp_init(seed)
     p = ctx.mlp_params()
     p[B3] = float(ys.mean())
     ctx.mlp_params(p)
     losses = ctx.mlp_train(Xs, ys, steps, batch, lr)
-    yhat, _ = ctx.mlp_predict()  # tensor-core path, the one queries use
-    res = y.astype(np.float64) - yhat
-    margin = float(np.quantile(res, quantile))
+    # calibrate with the training forward over the same rows; the tensor-core
+    # path that queries use differs from it by far less than the 0.02 added
+    yhat = np.concatenate([ctx.mlp_forward(Xs[i:i + 1_000_000]) for i in range(0, ys.size, 1_000_000)])
+    res = ys.astype(np.float64) - yhat
+    margin = float(np.quantile(res, quantile)) + 0.02
     ctx.mlp_set_margin(margin)
     return {"losses": losses, "margin": margin, "quantile": quantile, "rows": int(ys.size),
             "residual_std": float(res.std()), "target_mean": float(y.mean())}
