@@ -229,6 +229,36 @@ def run_ours(a):
                         "final_loss": float(rep["losses"][-20:].mean()), "first_loss": float(rep["losses"][:20].mean()),
                         "margin_log2": rep["margin"], "residual_std": rep["residual_std"],
                         "held_out_seed": 101 + rank}
+    compat = None
+    if not a.no_compat:
+        # the reference's own search and covariance, bit-identical neighbour
+        # lists, on the GPU (device-resident inputs, same flush between steps)
+        with Context(code_bits=wl["code_bits"], device=local, stream=stream.cuda_stream, search_compat=True) as cc:
+            out_c = torch.empty((u, 3), dtype=torch.float32, device="cuda")
+
+            def step_compat():
+                cc.build(dx, dy, dz)
+                cc.normals(k, out=out_c)
+
+            for _ in range(a.warmup):
+                step_compat()
+            n_c = max(3, min(a.steps, 5))
+            cprofs = []
+            evs = []
+            for i in range(n_c):
+                flush.fill_(float(i))
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                step_compat()
+                e1.record(stream)
+                evs.append((e0, e1))
+                cprofs.append(cc.profile())
+            torch.cuda.synchronize()
+            ms_c = sum(e0.elapsed_time(e1) for e0, e1 in evs)
+            compat = {"value": u * n_c / (ms_c * 1e-3), "ms_per_step": ms_c / n_c, "steps": n_c,
+                      "knn_normals_ms": statistics.mean(p["query_ms"] for p in cprofs),
+                      "desc": "reference search (face-plane box distance, 32-slot node heap) and FP32 "
+                              "covariance, neighbour lists identical to the reference build's; one GPU"}
     head = lrn if lrn is not None else plain
     ms_dev, ms_e2e, profs, stats, clocks = head["ms_dev"], head["ms_e2e"], head["profs"], head["stats"], head["clocks"]
 
@@ -284,6 +314,7 @@ def run_ours(a):
                 "knn_normals_ms": statistics.mean(p["query_ms"] for p in lrn["profs"]),
                 "misses_per_query": lrn["stats"]["learned_misses"] / max(u, 1),
                 "skip_seed": not a.learned_keep_seed, **lrn["train"]},
+            "compat": compat,
             "stages_ms": {**build_ms, "knn_normals": q_ms},
             "gpu_launches": int(launches),
             "fp64_solves_last_step": stats["fp64_solves"],
@@ -521,6 +552,7 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=200_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-cuda", action="store_true")
+    ap.add_argument("--no-compat", action="store_true", help="skip the reference-compatible search timing")
     ap.add_argument("--no-learned", action="store_true", help="time only the plain search")
     ap.add_argument("--learned-keep-seed", action="store_true",
                     help="with the learned radius, still offer the Morton-window seed")

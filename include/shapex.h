@@ -58,7 +58,14 @@ typedef struct se_options {
     int32_t learned;       /* 1: queries start from the learned radius (se_mlp_*);
                               queries it underestimates are searched again without it */
     int32_t learned_skip_seed; /* with learned: skip the Morton-window seed */
-    int32_t reserved[5];
+    int32_t search_compat; /* 1: se_knn, se_knn_self and se_normals run the reference's
+                              own approximate search (knnSearchKernel<k>,
+                              src/Octree.hpp:136-193: face-plane node distance,
+                              32-slot bounded node heap, k-slot result heap) and its
+                              FP32 covariance (src/NormalEstimation.hpp:96-120),
+                              reproducing its neighbour lists bit for bit; needs the
+                              octree (build_octree = 1); not with se_normals_batch */
+    int32_t reserved[4];
 } se_options;
 
 /* Sizes after se_build (RT::RadixTree / OT::Octree public fields). */

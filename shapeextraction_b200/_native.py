@@ -46,7 +46,8 @@ class SeOptions(ctypes.Structure):
         ("code_bits", ctypes.c_int32), ("root_compat", ctypes.c_int32), ("build_octree", ctypes.c_int32),
         ("viewpoint", ctypes.c_float * 3), ("eigengap_fp64", ctypes.c_float), ("leaf_bucket", ctypes.c_int32),
         ("device", ctypes.c_int32), ("stream", ctypes.c_void_p), ("seed_halo", ctypes.c_int32),
-        ("learned", ctypes.c_int32), ("learned_skip_seed", ctypes.c_int32), ("reserved", ctypes.c_int32 * 5),
+        ("learned", ctypes.c_int32), ("learned_skip_seed", ctypes.c_int32), ("search_compat", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 4),
     ]
 
 
@@ -161,7 +162,7 @@ class Context:
 
     def __init__(self, code_bits=63, root_compat=True, build_octree=True, viewpoint=(0.0, 0.0, 0.0),
                  eigengap_fp64=1e-4, leaf_bucket=32, device=0, stream=None, seed_halo=16, learned=False,
-                 learned_skip_seed=False):
+                 learned_skip_seed=False, search_compat=False):
         L = lib()
         o = SeOptions()
         L.se_options_init(ctypes.byref(o))
@@ -177,6 +178,7 @@ class Context:
         o.seed_halo = int(seed_halo)
         o.learned = int(bool(learned))
         o.learned_skip_seed = int(bool(learned_skip_seed))
+        o.search_compat = int(bool(search_compat))
         self.options = o
         h = ctypes.c_void_p()
         rc = L.se_create(ctypes.byref(h), ctypes.byref(o))

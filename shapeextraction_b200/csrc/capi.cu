@@ -223,7 +223,11 @@ int run_query(se_ctx* c, int k, int64_t start, int64_t count, const float* ext, 
     q.code_bits = c->opt.code_bits;
     q.bucket = c->opt.leaf_bucket;
     q.seed_halo = c->opt.seed_halo;
-    const bool use_learned = c->opt.learned && !ext && c->mlp_ready;
+    q.compat = c->opt.search_compat ? 1 : 0;
+    q.n_octree = c->info.n_octree;
+    if (q.compat && q.n_octree < 1)
+        return fail(c, SE_ERR_UNSUPPORTED, "the reference-compatible search needs the octree (build_octree = 1, u >= 2)");
+    const bool use_learned = c->opt.learned && !ext && c->mlp_ready && !q.compat;
     if (use_learned && c->r2_cap < count) {
         SE_CUDA(c, regrow(c->r2_buf, count), "alloc learned bounds");
         c->r2_cap = count;
@@ -324,6 +328,7 @@ int se_options_init(se_options* o) {
     o->seed_halo = 16;
     o->learned = 0;
     o->learned_skip_seed = 0;
+    o->search_compat = 0;
     return SE_OK;
 }
 
@@ -913,6 +918,8 @@ int se_normals_batch(se_ctx* c, const float* x, const float* y, const float* z, 
         return fail(c, SE_ERR_INVALID_ARG, "bad batch description");
     if (n_clouds == 0) return SE_OK;
     if (offsets[0] != 0) return fail(c, SE_ERR_INVALID_ARG, "offsets[0] must be 0");
+    if (c->opt.search_compat)
+        return fail(c, SE_ERR_UNSUPPORTED, "the reference-compatible search is not available in batches");
     for (int i = 0; i < n_clouds; ++i) {
         if (offsets[i + 1] < offsets[i]) return fail(c, SE_ERR_INVALID_ARG, "offsets must not decrease");
         if (ks[i] < 1 || ks[i] > 32) return fail(c, SE_ERR_UNSUPPORTED, "k must be in [1, 32]");

@@ -179,8 +179,13 @@ struct QueryParams {
     int learned_skip_seed;    // with learned_r2: skip the Morton-window seed
     int device_count;         // 1: query all u points of the build, u read on the device; `count`
                               // is then an upper bound used only to size the grid
+    int compat;               // 1: the reference's approximate octree search and FP32 covariance
+    int64_t n_octree;         // octree nodes (compat search)
 };
 
 cudaError_t enqueue_query(const BuildBufs& b, const QueryParams& q, cudaStream_t s, int num_sms);
+// Reference-compatible search over the OTNode array (enqueue_query forwards
+// to it when q.compat is set).
+cudaError_t enqueue_query_compat(const BuildBufs& b, const QueryParams& q, cudaStream_t s);
 
 }  // namespace shapex

@@ -251,3 +251,53 @@ def test_reference_api_facade(native, oracle):
     assert np.array_equal(oc.h_points, ref["points"])
     ei, _ = oracle.knn_exact(ref["points"], ref["points"][:100], 8)
     assert np.array_equal(oc.knnSearch(ref["points"][:100], 8), ei)
+
+
+COMPAT_CLOUDS = [
+    ("scene_200k_k16", lambda: synth.scene(200_000, 21), 16),
+    ("cube_100k_k10", lambda: synth.uniform_cube(100_000, 22), 10),
+    ("dups_20k_k8", lambda: synth.tiny_cloud(20_000, 23), 8),
+    ("mix_60k_k32", lambda: synth.precision_mix(60_000, 24), 32),
+]
+
+
+@pytest.mark.parametrize("name,gen,k", COMPAT_CLOUDS, ids=[c[0] for c in COMPAT_CLOUDS])
+def test_compat_search_bit_exact(native, oracle, name, gen, k):
+    """Reference-compatible search mode: the reference's approximate neighbour
+    lists (order included), self and external queries, against the oracle's
+    restatement; normals against the restated reference pipeline."""
+    x, y, z = gen()
+    with _ctx(native, search_compat=True) as c:
+        c.build(x, y, z)
+        nodes = c.octree()
+        pts = c.points()
+        idx = c.knn_self(k)
+        assert np.array_equal(idx, oracle.knn_compat(nodes, pts, pts, k))
+        rng = np.random.default_rng(5)
+        q = rng.uniform(-0.1, 1.1, (5000, 3)).astype(np.float32)
+        q[:2500] = pts[rng.choice(pts.shape[0], 2500)] + rng.normal(0, 1e-3, (2500, 3)).astype(np.float32)
+        assert np.array_equal(c.knn(q, k), oracle.knn_compat(nodes, pts, q, k))
+        nrm = c.normals(k)
+    u, ref = oracle.pipeline_reference(x, y, z, k)
+    assert u == pts.shape[0]
+    # both solve the same FP32 covariance in FP64; only (near-)repeated
+    # eigenvalues leave the direction free
+    _, ev = oracle.normals_f64(pts, idx, pts)
+    gap = (ev[:, 1] - ev[:, 0]) / np.maximum(ev[:, 2], 1e-300)
+    ok = gap > 1e-4
+    assert ok.mean() > 0.5
+    assert angle_deg_free(nrm[ok], ref[ok]).max() < 1e-4
+    d = np.sum(-pts[ok].astype(np.float64) * ref[ok], axis=1)
+    clear = np.abs(d) > 1e-4
+    assert np.all(np.sum(nrm[ok][clear] * ref[ok][clear], axis=1) > 0)
+
+
+def test_compat_search_rejections(native):
+    x, y, z = synth.uniform_cube(1000, 3)
+    with _ctx(native, search_compat=True, build_octree=False) as c:
+        c.build(x, y, z)
+        with pytest.raises(native.ShapexError):
+            c.knn_self(8)
+    with _ctx(native, search_compat=True) as c:
+        with pytest.raises(native.ShapexError):
+            c.normals_batch([(x, y, z)], np.array([8], np.int32))
