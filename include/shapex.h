@@ -65,7 +65,11 @@ typedef struct se_options {
                               FP32 covariance (src/NormalEstimation.hpp:96-120),
                               reproducing its neighbour lists bit for bit; needs the
                               octree (build_octree = 1); not with se_normals_batch */
-    int32_t reserved[4];
+    int32_t batch_graph;   /* 1: se_normals_batch records its launches once as a CUDA
+                              graph and replays it while the batch layout, the k's and
+                              the buffers repeat (inputs in device or pinned host
+                              memory); 0: plain stream launches every call */
+    int32_t reserved[3];
 } se_options;
 
 /* Sizes after se_build (RT::RadixTree / OT::Octree public fields). */
@@ -161,10 +165,14 @@ int se_normals(se_ctx* ctx, int k, int64_t start, int64_t count, float* out_xyz,
 /* Batched normal estimation over n_clouds independent clouds; no counterpart
  * in the reference (one cloud per call there). The clouds are concatenated
  * SoA: cloud c is points [offsets[c], offsets[c+1]) of x, y, z, with its own
- * k = ks[c] (1..32). Every cloud runs the whole path (bbox, codes, sort,
- * dedup, radix tree, search hierarchy, exact kNN, normals; no octree) with
- * device-side sizes, spread largest-first over the context's internal streams
- * with no host synchronisation between clouds. out_normals holds
+ * k = ks[c] (1..32). Every cloud's build (bbox, codes, sort, dedup, radix
+ * tree, search hierarchy; no octree) runs with device-side sizes, spread
+ * largest-first over the context's internal streams with no host
+ * synchronisation between clouds; then one persistent kNN + normals launch
+ * per distinct k serves all clouds with that k, warps taking 32-query items
+ * of the largest clouds first. With options.batch_graph the whole sequence is
+ * captured once as a CUDA graph and replayed by later calls with the same
+ * layout. out_normals holds
  * offsets[n_clouds] rows of xyz: cloud c's u_c normals (its unique points in
  * Morton order) start at row offsets[c]; out_u[c] = u_c. offsets, ks and out_u
  * are host arrays; x, y, z and out_normals follow `mem`. */

@@ -47,7 +47,7 @@ class SeOptions(ctypes.Structure):
         ("viewpoint", ctypes.c_float * 3), ("eigengap_fp64", ctypes.c_float), ("leaf_bucket", ctypes.c_int32),
         ("device", ctypes.c_int32), ("stream", ctypes.c_void_p), ("seed_halo", ctypes.c_int32),
         ("learned", ctypes.c_int32), ("learned_skip_seed", ctypes.c_int32), ("search_compat", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 4),
+        ("batch_graph", ctypes.c_int32), ("reserved", ctypes.c_int32 * 3),
     ]
 
 
@@ -162,7 +162,7 @@ class Context:
 
     def __init__(self, code_bits=63, root_compat=True, build_octree=True, viewpoint=(0.0, 0.0, 0.0),
                  eigengap_fp64=1e-4, leaf_bucket=32, device=0, stream=None, seed_halo=16, learned=False,
-                 learned_skip_seed=False, search_compat=False):
+                 learned_skip_seed=False, search_compat=False, batch_graph=True):
         L = lib()
         o = SeOptions()
         L.se_options_init(ctypes.byref(o))
@@ -179,6 +179,7 @@ class Context:
         o.learned = int(bool(learned))
         o.learned_skip_seed = int(bool(learned_skip_seed))
         o.search_compat = int(bool(search_compat))
+        o.batch_graph = int(bool(batch_graph))
         self.options = o
         h = ctypes.c_void_p()
         rc = L.se_create(ctypes.byref(h), ctypes.byref(o))

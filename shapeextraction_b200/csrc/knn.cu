@@ -10,14 +10,14 @@
 //
 // One warp serves 32 consecutive queries (Morton-ordered, so spatially
 // coherent); lane i owns query i. Each lane keeps its k best (squared
-// distance, index) keys in a max-heap in shared memory, whose root is the
-// lane's pruning bound. The warp first offers the Morton window around its
+// distance, index) keys as a sorted list in registers, whose last entry is
+// the lane's pruning bound. The warp first offers the Morton window around its
 // queries, then walks the search hierarchy depth first with a shared stack: a
 // child is entered when any lane's bound reaches its box, nearer child first
 // by lane vote. Bucket points (contiguous runs of at most `bucket` points) are
 // staged in shared memory and read by broadcast. A point that reaches a lane's
 // bound goes to that lane's candidate buffer; buffers are merged into the
-// heaps in batches, so that the warp pays for one heap update per buffered
+// lists in batches, so that the warp pays for one list update per buffered
 // slot rather than one per point any lane accepts. Pruning uses the box
 // distance with the same rounding chain as the point distance, so the result
 // is exact, ties broken by point index.
@@ -213,7 +213,7 @@ __device__ __forceinline__ void neu_add(float& s, float& c, float x) {
     s = t;
 }
 
-// Normal of one query from its k neighbours (heap[0..k), ascending):
+// Normal of one query from its k neighbours (nbr[0..k), ascending):
 // centred covariance with compensated FP32 sums, FP32 Jacobi, FP64 redo when
 // the relative eigengap (l1 - l0) / l2 is below `gap`, orientation towards
 // the viewpoint (src/NormalEstimation.hpp:184-189).
@@ -293,15 +293,13 @@ __device__ __forceinline__ void estimate_normal(const int32_t (&nbr)[K], int k, 
     out[2] = nz;
 }
 
+// The 32 queries [q0, q0 + 32) of one warp: search, then the outputs.
 template <int K, bool EXACT, bool EXT, bool NORMALS>
-__global__ void __launch_bounds__(kKnnThreads) k_knn(const float4* __restrict__ pts, const SNode* __restrict__ snodes,
-                                                     const uint64_t* __restrict__ codes, QArgs a, DevState* st) {
-    extern __shared__ __align__(16) unsigned char knn_smem[];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    WarpSmem& W = reinterpret_cast<WarpSmem*>(knn_smem)[warp];
+__device__ __forceinline__ void knn_warp(const float4* __restrict__ pts, const SNode* __restrict__ snodes,
+                                         const uint64_t* __restrict__ codes, const QArgs& a, DevState* st,
+                                         int64_t q0, WarpSmem& W, int lane) {
     const int64_t u = a.device_count ? (int64_t)st->u : a.u;
     const int64_t count = a.device_count ? u : a.count;
-    const int64_t q0 = ((int64_t)blockIdx.x * kKnnWarps + warp) * 32;
     if (q0 >= count) return;  // whole warp
     const int64_t qo = q0 + lane;
     const bool active = qo < count;
@@ -510,6 +508,48 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn(const float4* __restrict__ 
 }
 
 template <int K, bool EXACT, bool EXT, bool NORMALS>
+__global__ void __launch_bounds__(kKnnThreads) k_knn(const float4* __restrict__ pts, const SNode* __restrict__ snodes,
+                                                     const uint64_t* __restrict__ codes, QArgs a, DevState* st) {
+    extern __shared__ __align__(16) unsigned char knn_smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    WarpSmem& W = reinterpret_cast<WarpSmem*>(knn_smem)[warp];
+    const int64_t q0 = ((int64_t)blockIdx.x * kKnnWarps + warp) * 32;
+    knn_warp<K, EXACT, EXT, NORMALS>(pts, snodes, codes, a, st, q0, W, lane);
+}
+
+// Persistent kernel over many clouds that share k: each warp takes the next
+// 32-query item from a global counter until all are taken. Items are laid out
+// cloud by cloud in the order of `clouds` (largest first), so the large clouds
+// start first and the small ones fill the tail. Each cloud's size is read on
+// the device from its own build state.
+template <int K, bool EXACT>
+__global__ void __launch_bounds__(kKnnThreads) k_knn_batch(const BatchCloud* __restrict__ clouds, int n_clouds,
+                                                           int64_t n_items, unsigned long long* counter, QArgs a) {
+    extern __shared__ __align__(16) unsigned char knn_smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    WarpSmem& W = reinterpret_cast<WarpSmem*>(knn_smem)[warp];
+    for (;;) {
+        unsigned long long item = 0;
+        if (lane == 0) item = atomicAdd(counter, 1ull);
+        item = __shfl_sync(FULL, item, 0);
+        if (item >= (unsigned long long)n_items) break;
+        int lo = 0, hi = n_clouds - 1;  // last cloud whose first item is <= item
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if ((unsigned long long)__ldg(&clouds[mid].item0) <= item) lo = mid;
+            else hi = mid - 1;
+        }
+        const BatchCloud d = clouds[lo];
+        QArgs ca = a;
+        ca.out_normals = d.out_normals;
+        ca.start = 0;
+        ca.device_count = 1;
+        knn_warp<K, EXACT, false, true>(d.pts, d.snodes, nullptr, ca, d.st, ((int64_t)item - d.item0) * 32, W, lane);
+        __syncwarp();
+    }
+}
+
+template <int K, bool EXACT, bool EXT, bool NORMALS>
 cudaError_t launch_one(const BuildBufs& b, const QArgs& a, unsigned blocks, cudaStream_t s) {
     constexpr int smem = (int)sizeof(WarpSmem) * kKnnWarps;
     cudaError_t e =
@@ -528,7 +568,69 @@ cudaError_t launch_k(const BuildBufs& b, const QArgs& a, bool ext, bool normals,
     return launch_one<K, EXACT, false, false>(b, a, blocks, s);
 }
 
+template <int K, bool EXACT>
+cudaError_t launch_batch(const BatchCloud* clouds, int n_clouds, int64_t n_items, unsigned long long* counter,
+                         const QArgs& a, cudaStream_t s, int num_sms) {
+    constexpr int smem = (int)sizeof(WarpSmem) * kKnnWarps;
+    cudaError_t e = cudaFuncSetAttribute(k_knn_batch<K, EXACT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_knn_batch<K, EXACT>, kKnnThreads, smem);
+    if (e != cudaSuccess) return e;
+    const int64_t want = (n_items + kKnnWarps - 1) / kKnnWarps;
+    const int64_t resident = (int64_t)(per_sm > 0 ? per_sm : 1) * num_sms;
+    const unsigned blocks = (unsigned)(want < resident ? want : resident);
+    e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s);
+    if (e != cudaSuccess) return e;
+    k_knn_batch<K, EXACT><<<blocks, kKnnThreads, smem, s>>>(clouds, n_clouds, n_items, counter, a);
+    return cudaGetLastError();
+}
+
 }  // namespace
+
+__global__ void k_batch_collect(const DevState* __restrict__ st, int n, unsigned long long* __restrict__ u_out,
+                                uint32_t* __restrict__ err_out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    u_out[i] = st[i].u;
+    err_out[i] = st[i].err;
+}
+
+cudaError_t enqueue_batch_collect(const DevState* st, int n, unsigned long long* u_out, uint32_t* err_out,
+                                  cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    k_batch_collect<<<(n + 127) / 128, 128, 0, s>>>(st, n, u_out, err_out);
+    return cudaGetLastError();
+}
+
+cudaError_t enqueue_query_batch(const BatchCloud* clouds, int n_clouds, int64_t n_items, unsigned long long* counter,
+                                const QueryParams& q, cudaStream_t s, int num_sms) {
+    if (n_clouds <= 0 || n_items <= 0) return cudaSuccess;
+    if (q.k < 1 || q.k > 32) return cudaErrorInvalidValue;
+    QArgs a{};
+    a.k = q.k;
+    a.vx = q.vx;
+    a.vy = q.vy;
+    a.vz = q.vz;
+    a.gap = q.eigengap_fp64;
+    a.code_bits = q.code_bits;
+    a.bucket = q.bucket;
+    a.seed_halo = q.seed_halo < 0 ? 0 : (q.seed_halo > kMaxHalo ? kMaxHalo : q.seed_halo);
+    a.device_count = 1;
+    switch (q.k) {
+        case 8: return launch_batch<8, true>(clouds, n_clouds, n_items, counter, a, s, num_sms);
+        case 10: return launch_batch<10, true>(clouds, n_clouds, n_items, counter, a, s, num_sms);
+        case 16: return launch_batch<16, true>(clouds, n_clouds, n_items, counter, a, s, num_sms);
+        case 32: return launch_batch<32, true>(clouds, n_clouds, n_items, counter, a, s, num_sms);
+        default: break;
+    }
+    if (q.k <= 4) return launch_batch<4, false>(clouds, n_clouds, n_items, counter, a, s, num_sms);
+    if (q.k <= 8) return launch_batch<8, false>(clouds, n_clouds, n_items, counter, a, s, num_sms);
+    if (q.k <= 12) return launch_batch<12, false>(clouds, n_clouds, n_items, counter, a, s, num_sms);
+    if (q.k <= 16) return launch_batch<16, false>(clouds, n_clouds, n_items, counter, a, s, num_sms);
+    if (q.k <= 24) return launch_batch<24, false>(clouds, n_clouds, n_items, counter, a, s, num_sms);
+    return launch_batch<32, false>(clouds, n_clouds, n_items, counter, a, s, num_sms);
+}
 
 cudaError_t enqueue_query(const BuildBufs& b, const QueryParams& q, cudaStream_t s, int /*num_sms*/) {
     if (q.count <= 0) return cudaSuccess;

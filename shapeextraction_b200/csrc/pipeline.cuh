@@ -184,6 +184,29 @@ struct QueryParams {
 };
 
 cudaError_t enqueue_query(const BuildBufs& b, const QueryParams& q, cudaStream_t s, int num_sms);
+
+// One cloud of a batched query: its own points, search hierarchy and build
+// state (u is read there on the device), its output, and the index of its
+// first 32-query item in the launch.
+struct BatchCloud {
+    const float4* pts;
+    const SNode* snodes;
+    DevState* st;
+    float* out_normals;
+    int64_t item0;
+};
+
+// Normals of many clouds that share q.k in one persistent launch (grid = the
+// kernel's resident blocks on every SM). `clouds` is a device array of
+// n_clouds entries, `counter` a device word this call resets. q supplies k,
+// viewpoint, eigengap threshold, bucket and seed halo.
+// u and the error word of every cloud of a batch (states st[0..n)) into
+// u_out / err_out.
+cudaError_t enqueue_batch_collect(const DevState* st, int n, unsigned long long* u_out, uint32_t* err_out,
+                                  cudaStream_t s);
+
+cudaError_t enqueue_query_batch(const BatchCloud* clouds, int n_clouds, int64_t n_items, unsigned long long* counter,
+                                const QueryParams& q, cudaStream_t s, int num_sms);
 // Reference-compatible search over the OTNode array (enqueue_query forwards
 // to it when q.compat is set).
 cudaError_t enqueue_query_compat(const BuildBufs& b, const QueryParams& q, cudaStream_t s);

@@ -42,7 +42,7 @@ def test_options_defaults(native):
     assert L.se_options_init(ctypes.byref(o)) == 0
     assert o.code_bits == 63 and o.root_compat == 1 and o.build_octree == 1
     assert tuple(o.viewpoint) == (0.0, 0.0, 0.0)
-    assert o.search_compat == 0 and o.learned == 0
+    assert o.search_compat == 0 and o.learned == 0 and o.batch_graph == 1
     assert ctypes.sizeof(o) == 80  # sizeof(se_options) in C: 17 four-byte fields, a pointer, 4 B padding
     assert L.se_abi_version() == 1
     assert L.se_status_string(5) == b"SE_ERR_NONFINITE"

@@ -59,3 +59,63 @@ def test_batch_rejects_bad_input(native):
         x = np.zeros(10, np.float32)
         with pytest.raises(native.ShapexError):
             c.normals_batch([(x, x, x)], np.array([40], np.int32))  # k > 32
+
+
+def test_batch_graph_replay_equals_direct_launches(native):
+    """The recorded graph (device or pinned host buffers) gives the same
+    normals as plain launches, on first recording, on replay, after a layout
+    change and when two layouts alternate."""
+    import torch
+
+    clouds, ks = _clouds(5, 17)
+    clouds2, ks2 = _clouds(6, 11)
+    with native.Context(batch_graph=False) as c:
+        ref, offsets, u = c.normals_batch(clouds, ks)
+        ref2, offsets2, u2 = c.normals_batch(clouds2, ks2)
+    host = [torch.from_numpy(np.concatenate([cl[j] for cl in clouds])).pin_memory() for j in range(3)]
+    host2 = [torch.from_numpy(np.concatenate([cl[j] for cl in clouds2])).pin_memory() for j in range(3)]
+    dev = [h.cuda() for h in host]
+    with native.Context(batch_graph=True) as c:
+        out_h = torch.zeros((int(offsets[-1]), 3), dtype=torch.float32).pin_memory()
+        out_h2 = torch.zeros((int(offsets2[-1]), 3), dtype=torch.float32).pin_memory()
+        for rep in range(3):
+            out_h.zero_()
+            _, _, uu = c.normals_batch(tuple(host), (ks, offsets), out=out_h)
+            assert np.array_equal(uu, u)
+            assert np.array_equal(out_h.numpy(), ref), rep
+            out_h2.zero_()
+            _, _, uu2 = c.normals_batch(tuple(host2), (ks2, offsets2), out=out_h2)
+            assert np.array_equal(uu2, u2)
+            assert np.array_equal(out_h2.numpy(), ref2), rep
+            d, _, uu = c.normals_batch(tuple(dev), (ks, offsets))
+            assert np.array_equal(d.cpu().numpy(), ref), rep
+        prof = c.profile()
+        assert prof["query_launches"] == len(set(ks[u > 0].tolist())) + 1
+
+
+@pytest.mark.parametrize("graph", [True, False])
+def test_batch_large_and_small_clouds(native, graph):
+    """Clouds large enough to be queried on their build lane next to small
+    ones that share the persistent launch: every cloud equals its
+    single-cloud call, through plain launches and through the graph."""
+    import torch
+
+    sizes = [150_000, 70_000, 3000, 500, 65_536, 65_535, 1, 0, 20_000]
+    ks = np.array([16, 32, 8, 16, 10, 16, 8, 16, 5], np.int32)
+    clouds = [synth.scene(s, seed=300 + i) if s > 0 else (np.zeros(0, np.float32),) * 3 for i, s in enumerate(sizes)]
+    offsets = np.zeros(len(sizes) + 1, np.int64)
+    offsets[1:] = np.cumsum(sizes)
+    host = [torch.from_numpy(np.concatenate([cl[j] for cl in clouds])).pin_memory() for j in range(3)]
+    with native.Context(batch_graph=graph) as c:
+        out = torch.zeros((int(offsets[-1]), 3), dtype=torch.float32).pin_memory()
+        for _ in range(2):
+            out.zero_()
+            _, _, u = c.normals_batch(tuple(host), (ks, offsets), out=out)
+        nrm = out.numpy().copy()
+        for i, (x, y, z) in enumerate(clouds):
+            if x.size == 0:
+                assert u[i] == 0
+                continue
+            c.build(x, y, z)
+            assert u[i] == c.info()["n_points"]
+            assert np.array_equal(nrm[offsets[i]:offsets[i] + u[i]], c.normals(int(ks[i]))), i
