@@ -45,8 +45,9 @@ def _workloads():
     return {
         "scene_2M_k16": dict(gen=lambda s: synth.scene(2_000_000, s), k=16, code_bits=63,
                              desc="2M points on 32 spheres + 8 planes, jitter 0.002, 63-bit codes, k=16"),
-        "precision_20M_k16": dict(gen=lambda s: synth.precision_mix(20_000_000, s), k=16, code_bits=63,
-                                  desc="20M points precision mix, 63-bit codes, k=16"),
+        "precision_20M_k16": dict(gen=lambda s: synth.precision_mix(20_000_000, s), k=16, code_bits=63, eigengap=1e-6,
+                                  desc="20M points precision mix, 63-bit codes, k=16, FP64 eigensolve below a "
+                                       "relative eigengap of 1e-6"),
         "gmm_50M_k16": dict(gen=lambda s: synth.gaussian_mixture(50_000_000, s), k=16, code_bits=63,
                             desc="50M points Gaussian mixture + surfaces, 63-bit codes, k=16"),
         "cube_100k_k10": dict(gen=lambda s: synth.uniform_cube(100_000, s), k=10, code_bits=30,
@@ -548,7 +549,8 @@ def main():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--bucket", type=int, default=32)
     ap.add_argument("--halo", type=int, default=16)
-    ap.add_argument("--eigengap", type=float, default=1e-4)
+    ap.add_argument("--eigengap", type=float, default=None,
+                    help="FP64-redo eigengap threshold (default: the workload's, else 1e-4)")
     ap.add_argument("--cpu-sample", type=int, default=200_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-cuda", action="store_true")
@@ -562,6 +564,8 @@ def main():
     a = ap.parse_args()
     if a.warmup < 3:
         a.warmup = 3
+    if a.eigengap is None:
+        a.eigengap = _workloads()[a.workload].get("eigengap", 1e-4)
     if a.impl == "reference":
         run_reference(a)
     elif _workloads()[a.workload].get("batched"):
