@@ -304,8 +304,11 @@ __global__ void __launch_bounds__(128) k_predict_radius(const float* __restrict_
     }
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t q0 = ((int64_t)blockIdx.x * 4 + warp) * 32;
-    if (q0 >= count) return;
+    const float b3 = params[MlpLayout::B3];
+    // the block keeps its weights in shared memory and walks 128-query chunks
+    for (int64_t chunk = blockIdx.x;; chunk += gridDim.x) {
+    const int64_t q0 = (chunk * 4 + warp) * 32;
+    if (q0 >= count) break;
     const int64_t qo = q0 + lane;
     const bool active = qo < count;
     const float range = st->range;
@@ -352,7 +355,6 @@ __global__ void __launch_bounds__(128) k_predict_radius(const float* __restrict_
             y[mb][h] += __shfl_xor_sync(FULL, y[mb][h], 1);
             y[mb][h] += __shfl_xor_sync(FULL, y[mb][h], 2);
         }
-    const float b3 = params[MlpLayout::B3];
     // lane t == 0 of quad g holds rows g, g+8, g+16, g+24
     if (t == 0) {
 #pragma unroll
@@ -367,6 +369,8 @@ __global__ void __launch_bounds__(128) k_predict_radius(const float* __restrict_
                     if (r2_out) r2_out[o] = range * range * exp2f(yh + margin);
                 }
             }
+    }
+    __syncwarp();  // S.x / S.h of this warp are rewritten by its next chunk
     }
 }
 
@@ -385,7 +389,15 @@ cudaError_t enqueue_features(const BuildBufs& b, int64_t u, int code_bits, int64
 cudaError_t enqueue_predict_radius(const BuildBufs& b, const float* params, float margin, int64_t u, int code_bits,
                                    int64_t start, int64_t count, float* r2_out, float* yhat_out, cudaStream_t s) {
     if (count <= 0) return cudaSuccess;
-    const unsigned blocks = blocks_for((count + 31) / 32, 4);
+    // the resident blocks only, each loading the weights once
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_predict_radius, 128, 0);
+    if (e != cudaSuccess) return e;
+    const int64_t resident = (int64_t)(per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+    const int64_t want = (int64_t)blocks_for((count + 31) / 32, 4);
+    const unsigned blocks = (unsigned)(want < resident ? want : resident);
     k_predict_radius<<<blocks, 128, 0, s>>>(params, margin, b.pts4, b.leaf_parent, b.sparent, b.prefix_n, b.range_end,
                                             b.codes, u, code_bits, start, count, r2_out, yhat_out, b.st);
     return cudaGetLastError();
