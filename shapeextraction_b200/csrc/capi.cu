@@ -278,6 +278,21 @@ int run_query(se_ctx* c, int k, int64_t start, int64_t count, const float* ext, 
             q.ext_queries = ext;
         }
     }
+    // Pinned host outputs are written by the kernel itself (mapped host
+    // memory), so the results cross PCIe while the kernel runs instead of in
+    // a copy after it. Other host outputs go through device staging.
+    auto mapped = [&](void* p) -> void* {
+        if (!host || !p) return nullptr;
+        cudaPointerAttributes at{};
+        if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        return at.type == cudaMemoryTypeHost ? at.devicePointer : nullptr;
+    };
+    void* m_idx = mapped(out_idx);
+    void* m_d2 = mapped(out_d2);
+    void* m_nrm = mapped(out_normals);
     if (out_idx) {
         if (host) {
             if (c->idx_cap < (int64_t)k * count) {
@@ -285,8 +300,8 @@ int run_query(se_ctx* c, int k, int64_t start, int64_t count, const float* ext, 
                 SE_CUDA(c, regrow(c->d2_buf, (int64_t)k * count), "alloc knn staging");
                 c->idx_cap = (int64_t)k * count;
             }
-            q.out_idx = c->idx_buf;
-            q.out_d2 = out_d2 ? c->d2_buf : nullptr;
+            q.out_idx = m_idx ? static_cast<int32_t*>(m_idx) : c->idx_buf;
+            q.out_d2 = out_d2 ? (m_d2 ? static_cast<float*>(m_d2) : c->d2_buf) : nullptr;
         } else {
             q.out_idx = out_idx;
             q.out_d2 = out_d2;
@@ -298,7 +313,7 @@ int run_query(se_ctx* c, int k, int64_t start, int64_t count, const float* ext, 
                 SE_CUDA(c, regrow(c->out_buf, 3 * count), "alloc normals staging");
                 c->out_cap = 3 * count;
             }
-            q.out_normals = c->out_buf;
+            q.out_normals = m_nrm ? static_cast<float*>(m_nrm) : c->out_buf;
         } else {
             q.out_normals = out_normals;
         }
@@ -314,20 +329,20 @@ int run_query(se_ctx* c, int k, int64_t start, int64_t count, const float* ext, 
                 "launch radius prediction");
     SE_CUDA(c, enqueue_query(c->b, q, c->stream, c->num_sms), "launch query");
     SE_CUDA(c, cudaEventRecord(c->query_ev[1], c->stream), "event");
-    c->query_launches = use_learned ? 2 : 1;
-    c->have_query_times = true;
     if (host) {
-        if (out_idx)
+        if (out_idx && q.out_idx == c->idx_buf)
             SE_CUDA(c, cudaMemcpyAsync(out_idx, q.out_idx, sizeof(int32_t) * k * count, cudaMemcpyDeviceToHost, c->stream),
                     "copy knn");
-        if (out_idx && out_d2)
+        if (out_idx && out_d2 && q.out_d2 == c->d2_buf)
             SE_CUDA(c, cudaMemcpyAsync(out_d2, q.out_d2, sizeof(float) * k * count, cudaMemcpyDeviceToHost, c->stream),
                     "copy knn");
-        if (out_normals)
+        if (out_normals && q.out_normals == c->out_buf)
             SE_CUDA(c, cudaMemcpyAsync(out_normals, q.out_normals, sizeof(float) * 3 * count, cudaMemcpyDeviceToHost,
                                        c->stream),
                     "copy normals");
     }
+    c->query_launches = use_learned ? 2 : 1;
+    c->have_query_times = true;
     SE_CUDA(c, cudaMemcpyAsync(&c->h_st->err, &c->b.st->err, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream),
             "read state");
     SE_CUDA(c, cudaMemcpyAsync(c->h_st->counters, c->b.st->counters, sizeof(c->b.st->counters),

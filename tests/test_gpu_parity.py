@@ -301,3 +301,32 @@ def test_compat_search_rejections(native):
     with _ctx(native, search_compat=True) as c:
         with pytest.raises(native.ShapexError):
             c.normals_batch([(x, y, z)], np.array([8], np.int32))
+
+
+def test_pinned_host_outputs_equal_device_outputs(native):
+    """Pinned host outputs are written by the kernel directly (mapped host
+    memory); pageable ones go through device staging. Both equal the
+    device-output call bit for bit."""
+    import torch
+
+    x, y, z = synth.scene(300_000, 31)
+    with _ctx(native) as c:
+        u = c.build(x, y, z)["n_points"]
+        n_dev = torch.empty((u, 3), dtype=torch.float32, device="cuda")
+        c.normals(16, out=n_dev)
+        n_pin = torch.zeros((u, 3), dtype=torch.float32).pin_memory()
+        c.normals(16, out=n_pin)
+        assert np.array_equal(n_pin.numpy(), n_dev.cpu().numpy())
+        assert np.array_equal(c.normals(16), n_dev.cpu().numpy())  # pageable numpy output
+        i_dev = torch.empty((u, 10), dtype=torch.int32, device="cuda")
+        d_dev = torch.empty((u, 10), dtype=torch.float32, device="cuda")
+        c.knn_self(10, out=i_dev, out_d2=d_dev)
+        i_pin = torch.zeros((u, 10), dtype=torch.int32).pin_memory()
+        d_pin = torch.zeros((u, 10), dtype=torch.float32).pin_memory()
+        c.knn_self(10, out=i_pin, out_d2=d_pin)
+        assert np.array_equal(i_pin.numpy(), i_dev.cpu().numpy()) and np.array_equal(d_pin.numpy(), d_dev.cpu().numpy())
+        # a sub-range into the middle of a pinned buffer
+        part = torch.zeros((u, 3), dtype=torch.float32).pin_memory()
+        c.normals(16, 1000, 5000, out=part[1000:6000])
+        assert np.array_equal(part[1000:6000].numpy(), n_dev[1000:6000].cpu().numpy())
+        assert np.all(part[:1000].numpy() == 0) and np.all(part[6000:].numpy() == 0)
