@@ -1005,11 +1005,10 @@ int grow_batch(se_ctx* c, T*& p, int64_t count, const char* what) {
 // words, the host-output copies.
 int enqueue_batch(se_ctx* c, const BatchPlan& plan, const BatchCloud* d_desc, const float* x, const float* y,
                   const float* z, const int64_t* offsets, int n_clouds, const int32_t* ks, float* out_normals,
-                  bool host, int& launches) {
+                  float* bout, bool host, int& launches) {
     const int64_t total = offsets[n_clouds];
     cudaStream_t g = c->graph_stream;
     const float *bx = x, *by = y, *bz = z;
-    float* bout = out_normals;
     if (host && total > 0) {
         SE_CUDA(c, cudaMemcpyAsync(c->batch_in, x, 4 * total, cudaMemcpyHostToDevice, g), "copy x");
         SE_CUDA(c, cudaMemcpyAsync(c->batch_in + total, y, 4 * total, cudaMemcpyHostToDevice, g), "copy y");
@@ -1017,7 +1016,6 @@ int enqueue_batch(se_ctx* c, const BatchPlan& plan, const BatchCloud* d_desc, co
         bx = c->batch_in;
         by = c->batch_in + total;
         bz = c->batch_in + 2 * total;
-        bout = c->batch_out;
     }
     for (int ci = 0; ci < n_clouds; ++ci)
         if (offsets[ci + 1] == offsets[ci]) {  // empty cloud: no build clears its state
@@ -1090,7 +1088,7 @@ int enqueue_batch(se_ctx* c, const BatchPlan& plan, const BatchCloud* d_desc, co
     }
     SE_CUDA(c, enqueue_batch_collect(c->batch_st, n_clouds, c->batch_u, c->batch_err, g), "launch batch collect");
     ++launches;
-    if (host && total > 0)
+    if (host && total > 0 && bout == c->batch_out)  // staged (pageable) host output
         SE_CUDA(c, cudaMemcpyAsync(out_normals, bout, sizeof(float) * 3 * total, cudaMemcpyDeviceToHost, g),
                 "copy normals");
     SE_CUDA(c, cudaMemcpyAsync(c->h_batch_u, c->batch_u, sizeof(unsigned long long) * n_clouds, cudaMemcpyDeviceToHost,
@@ -1226,7 +1224,17 @@ int se_normals_batch(se_ctx* c, const float* x, const float* y, const float* z, 
         }
     }
     std::vector<BatchCloud> desc;
-    float* bout = host ? c->batch_out : out_normals;
+    // a pinned host output is written by the kernels directly (mapped memory)
+    float* bout = out_normals;
+    if (host && total > 0) {
+        bout = c->batch_out;
+        cudaPointerAttributes at{};
+        if (cudaPointerGetAttributes(&at, out_normals) == cudaSuccess) {
+            if (at.type == cudaMemoryTypeHost && at.devicePointer) bout = static_cast<float*>(at.devicePointer);
+        } else {
+            cudaGetLastError();
+        }
+    }
     for (int k : plan.group_k) {
         plan.group_first.push_back((int)desc.size());
         int64_t items = 0;
@@ -1300,7 +1308,8 @@ int se_normals_batch(se_ctx* c, const float* x, const float* y, const float* z, 
                 release_graph(bg);
                 return cuda_fail(c, ce, "begin capture");
             }
-            const int rc = enqueue_batch(c, plan, d_desc, x, y, z, offsets, n_clouds, ks, out_normals, host, launches);
+            const int rc =
+                enqueue_batch(c, plan, d_desc, x, y, z, offsets, n_clouds, ks, out_normals, bout, host, launches);
             cudaGraph_t graph = nullptr;
             ce = cudaStreamEndCapture(c->graph_stream, &graph);
             if (rc == SE_OK && ce == cudaSuccess) ce = cudaGraphInstantiate(&bg.exec, graph, 0);
@@ -1313,7 +1322,8 @@ int se_normals_batch(se_ctx* c, const float* x, const float* y, const float* z, 
             c->batch_graphs.push_back(bg);
             SE_CUDA(c, cudaGraphLaunch(bg.exec, c->graph_stream), "launch batch graph");
         } else {
-            if (int rc = enqueue_batch(c, plan, d_desc, x, y, z, offsets, n_clouds, ks, out_normals, host, launches))
+            if (int rc =
+                    enqueue_batch(c, plan, d_desc, x, y, z, offsets, n_clouds, ks, out_normals, bout, host, launches))
                 return rc;
         }
     } else {
