@@ -464,12 +464,47 @@ def reference_cuda(workload, seed, reps=3):
     from shapeextraction_b200 import synth
 
     wl = _workloads()[workload]
+
+    def well_formed(x, y, z):
+        a = O.build_stages(x, y, z, 63, root_compat=True)["radix"]
+        b = O.build_stages(x, y, z, 63, root_compat=False)["radix"]
+        return all(np.array_equal(a[key][:1], b[key][:1]) for key in ("leftChild", "prefixN", "hasLeafLeft",
+                                                                         "hasLeafRight"))
+
     if wl.get("batched"):
-        return {"unavailable": "batched workload: the reference runs one cloud per process call"}
+        # the reference has no batched entry point: its API runs cloud after cloud
+        clouds, ks = wl["gen"](seed)
+        with tempfile.TemporaryDirectory() as tmp:
+            lines, skipped, n_in = [], 0, 0
+            for i, ((cx, cy, cz), kk) in enumerate(zip(clouds, ks)):
+                if cx.size < 3 or not well_formed(cx, cy, cz):
+                    skipped += 1
+                    continue
+                f = os.path.join(tmp, f"c{i}.bin")
+                synth.to_cloud_file(f, cx, cy, cz)
+                lines.append(f"{f} {int(kk)}")
+                n_in += cx.size
+            lst = os.path.join(tmp, "list.txt")
+            with open(lst, "w") as fh:
+                fh.write("\n".join(lines) + "\n")
+            try:
+                r = subprocess.run([exe, "batch", lst, "1", str(max(1, reps - 2))], capture_output=True, text=True,
+                                   timeout=1500)
+            except subprocess.TimeoutExpired:
+                return {"unavailable": "reference CUDA build exceeded 1500 s on the batch"}
+        lines = [ln for ln in r.stdout.splitlines() if ln.startswith("REFJSON ")]
+        if r.returncode != 0 or not lines:
+            return {"unavailable": f"refdriver exit {r.returncode}: {r.stderr[-300:]}"}
+        d = json.loads(lines[-1][8:])
+        ms = statistics.median(d["ms"])
+        return {"value": d["u"] / (ms * 1e-3), "unit": "normals/s", "ms": d["ms"], "u": d["u"], "clouds": d["clouds"],
+                "skipped_clouds": skipped, "points": n_in,
+                "span": "cloud after cloud: host PointCloud in -> RadixTree ctor -> Octree ctor -> "
+                        "estimateNormals<k> -> host normals",
+                "build": "unmodified reference sources, nvcc 12.9 -O3 -DNDEBUG sm_100a (oracle/build_ref.sh)",
+                "cuda_error": d.get("cuda_error")}
     x, y, z = wl["gen"](seed)
-    a = O.build_stages(x, y, z, 63, root_compat=True)["radix"]
-    b = O.build_stages(x, y, z, 63, root_compat=False)["radix"]
-    if not all(np.array_equal(a[key][:1], b[key][:1]) for key in ("leftChild", "prefixN", "hasLeafLeft", "hasLeafRight")):
+    if not well_formed(x, y, z):
         return {"unavailable": "the reference's root range breaks this cloud's tree (it would read unset parents)"}
     with tempfile.TemporaryDirectory() as tmp:
         f = os.path.join(tmp, "cloud.bin")

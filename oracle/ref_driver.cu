@@ -9,6 +9,10 @@
 //
 //   refdriver dump  <cloud.bin> <outdir> <k>
 //   refdriver bench <cloud.bin> <k> <warmup> <reps>
+//   refdriver batch <list.txt> <warmup> <reps>
+//       list.txt: one "<cloud.bin> <k>" per line; every rep runs the clouds
+//       one after another through the same API calls (the reference has no
+//       batched entry point) and reports the summed time.
 //
 // cloud.bin: int64 n, then n float32 x, n float32 y, n float32 z.
 // Only clouds whose radix tree the CPU oracle has checked to be well formed
@@ -102,9 +106,60 @@ static int bench(const PointCloud<float>& cloud, int warmup, int reps) {
     return 0;
 }
 
+template <int k>
+static int one_cloud(const PointCloud<float>& cloud) {
+    RT::RadixTree rt(cloud);
+    OT::Octree oct(rt);
+    std::vector<Point> normals = NormalEstimation::estimateNormals<k>(oct);
+    cudaDeviceSynchronize();
+    return oct.n_pts;
+}
+
+static int batch(const char* list, int warmup, int reps) {
+    std::vector<PointCloud<float>> clouds;
+    std::vector<int> ks;
+    FILE* f = std::fopen(list, "r");
+    if (!f) return 2;
+    char path[4096];
+    int k = 0;
+    while (std::fscanf(f, "%4095s %d", path, &k) == 2) {
+        clouds.emplace_back();
+        if (!read_cloud(path, clouds.back())) { std::fclose(f); return 2; }
+        ks.push_back(k);
+    }
+    std::fclose(f);
+    std::vector<double> ms;
+    long long u_total = 0;
+    for (int r = 0; r < warmup + reps; ++r) {
+        cudaDeviceSynchronize();
+        auto t0 = std::chrono::steady_clock::now();
+        long long u = 0;
+        for (size_t i = 0; i < clouds.size(); ++i) {
+            switch (ks[i]) {
+                case 8: u += one_cloud<8>(clouds[i]); break;
+                case 10: u += one_cloud<10>(clouds[i]); break;
+                case 16: u += one_cloud<16>(clouds[i]); break;
+                case 32: u += one_cloud<32>(clouds[i]); break;
+                default: return 2;
+            }
+        }
+        auto t1 = std::chrono::steady_clock::now();
+        u_total = u;
+        if (r >= warmup) ms.push_back(std::chrono::duration<double, std::milli>(t1 - t0).count());
+    }
+    std::printf("REFJSON {\"clouds\": %zu, \"u\": %lld, \"ms\": [", clouds.size(), u_total);
+    for (size_t i = 0; i < ms.size(); ++i) std::printf("%s%.4f", i ? ", " : "", ms[i]);
+    std::printf("], \"cuda_error\": \"%s\"}\n", cudaGetErrorString(cudaGetLastError()));
+    return 0;
+}
+
 int main(int argc, char** argv) {
     if (argc < 4) { std::fprintf(stderr, "usage: see header\n"); return 2; }
     const std::string mode = argv[1];
+    if (mode == "batch") {
+        if (argc < 5) return 2;
+        return batch(argv[2], std::atoi(argv[3]), std::atoi(argv[4]));
+    }
     PointCloud<float> cloud;
     if (!read_cloud(argv[2], cloud)) { std::fprintf(stderr, "cannot read %s\n", argv[2]); return 2; }
     if (mode == "dump") {
