@@ -43,16 +43,20 @@ def _workloads():
     from shapeextraction_b200 import synth
 
     return {
-        "scene_2M_k16": dict(gen=lambda s: synth.scene(2_000_000, s), k=16, code_bits=63,
+        "scene_2M_k16": dict(gen=lambda s: synth.scene(2_000_000, s), sample=synth.scene, k=16, code_bits=63,
                              desc="2M points on 32 spheres + 8 planes, jitter 0.002, 63-bit codes, k=16"),
-        "precision_20M_k16": dict(gen=lambda s: synth.precision_mix(20_000_000, s), k=16, code_bits=63, eigengap=1e-6,
+        "precision_20M_k16": dict(gen=lambda s: synth.precision_mix(20_000_000, s), sample=synth.precision_mix, k=16,
+                                  code_bits=63, eigengap=1e-6,
                                   desc="20M points precision mix, 63-bit codes, k=16, FP64 eigensolve below a "
                                        "relative eigengap of 1e-6"),
-        "gmm_50M_k16": dict(gen=lambda s: synth.gaussian_mixture(50_000_000, s), k=16, code_bits=63,
+        "gmm_50M_k16": dict(gen=lambda s: synth.gaussian_mixture(50_000_000, s), sample=synth.gaussian_mixture, k=16,
+                            code_bits=63,
                             desc="50M points Gaussian mixture + surfaces, 63-bit codes, k=16"),
-        "cube_100k_k10": dict(gen=lambda s: synth.uniform_cube(100_000, s), k=10, code_bits=30,
+        "cube_100k_k10": dict(gen=lambda s: synth.uniform_cube(100_000, s), sample=synth.uniform_cube, k=10,
+                              code_bits=30,
                               desc="100k uniform points, 30-bit codes, k=10"),
-        "batch_256": dict(gen=lambda s: synth.batched_clouds(256, s), k=None, code_bits=63, batched=True,
+        "batch_256": dict(gen=lambda s: synth.batched_clouds(256, s), sample=synth.scene, k=None, code_bits=63,
+                          batched=True,
                           desc="256 independent scenes, sizes log-uniform in [1k, 500k], k per cloud in {8,16,32}, "
                                "one se_normals_batch call"),
     }
@@ -410,7 +414,7 @@ def run_batch(a):
     achieved = alg / (ms_dev / a.steps * 1e-3) / 1e9
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        cpu = cpu_baseline("scene_2M_k16", a.seed, a.cpu_sample)
+        cpu = cpu_baseline(a.workload, a.seed, a.cpu_sample)
     if rank == 0:
         print(json.dumps({
             "metric": METRIC, "value": u_all * a.steps / (ms_dev * 1e-3), "unit": "normals/s", "n_gpus": world,
@@ -441,18 +445,17 @@ def cpu_baseline(workload, seed, sample):
     wl = _workloads()[workload]
     from shapeextraction_b200 import synth
 
-    if workload.startswith("cube"):
-        x, y, z = synth.uniform_cube(min(sample, 100_000), seed)
-    else:
-        x, y, z = synth.scene(sample, seed)
-    O.pipeline_reference(x[:1000], y[:1000], z[:1000], wl["k"])  # warm the library
+    k = wl["k"] or 16
+    n = min(sample, 100_000) if workload.startswith("cube") else sample
+    x, y, z = wl["sample"](n, seed)
+    O.pipeline_reference(x[:1000], y[:1000], z[:1000], k)  # warm the library
     t = time.perf_counter()
-    u, _ = O.pipeline_reference(x, y, z, wl["k"])
+    u, _ = O.pipeline_reference(x, y, z, k)
     dt = time.perf_counter() - t
     return {"value": u / dt, "unit": "normals/s", "cores": os.cpu_count(), "kind": "port",
-            "sample": f"{x.size} points of the same scene generator, k={wl['k']}: reference pipeline restated on "
-                      "the host (bit-exact build, the reference's approximate octree search, FP32 covariance, "
-                      "FP64 Jacobi), OpenMP on all cores", "seconds": dt}
+            "sample": f"{x.size} points of the workload's generator ({wl['sample'].__name__}), k={k}: reference "
+                      "pipeline restated on the host (bit-exact build, the reference's approximate octree search, "
+                      "FP32 covariance, FP64 Jacobi), OpenMP on all cores", "seconds": dt}
 
 
 def reference_cuda(workload, seed, reps=3):
@@ -534,10 +537,8 @@ def run_reference(a):
     from shapeextraction_b200 import synth
 
     k_ref = wl["k"] or 16
-    if a.workload.startswith("cube"):
-        x, y, z = synth.uniform_cube(min(a.cpu_sample, 100_000), a.seed)
-    else:
-        x, y, z = synth.scene(a.cpu_sample, a.seed)
+    n = min(a.cpu_sample, 100_000) if a.workload.startswith("cube") else a.cpu_sample
+    x, y, z = wl["sample"](n, a.seed)
     for _ in range(a.warmup):
         O.pipeline_reference(x, y, z, k_ref)
     times = []
@@ -548,8 +549,9 @@ def run_reference(a):
         times.append(time.perf_counter() - t)
     tot = sum(times)
     value = u * a.steps / tot
-    sample = (f"{x.size} points of the same scene generator per step, k={k_ref}: reference pipeline restated on "
-              "the host (bit-exact build, the reference's approximate octree search, FP32 covariance, FP64 Jacobi)")
+    sample = (f"{x.size} points of the workload's generator ({wl['sample'].__name__}) per step, k={k_ref}: reference "
+              "pipeline restated on the host (bit-exact build, the reference's approximate octree search, FP32 "
+              "covariance, FP64 Jacobi)")
     line = {
         "impl": "reference",
         "metric": METRIC,
