@@ -36,7 +36,15 @@ namespace {
 constexpr int kKnnThreads = 128;
 constexpr int kKnnWarps = kKnnThreads / 32;
 constexpr int kStackDepth = 96;
-constexpr int kBuf = 64;                // per-lane candidate buffer slots (point indices)
+// Per-k tile shape, measured on B200 (2M scene and 5M mixture clouds): small
+// lists leave registers for more resident warps, which pays for itself up to
+// k = 16; the 32-key list needs its registers (about 150), so it keeps the
+// larger buffer and 3 blocks per SM.
+template <int K>
+struct KnnCfg {
+    static constexpr int buf = K <= 8 ? 40 : (K <= 16 ? 48 : 64);  // candidate buffer slots per lane
+    static constexpr int min_blocks = K <= 8 ? 6 : (K <= 16 ? 5 : 3);  // resident 128-thread blocks per SM
+};
 constexpr int kMaxHalo = 48;            // seed points on each side of a warp's queries
 constexpr int kWindowMax = 32 + 2 * kMaxHalo;
 constexpr unsigned FULL = 0xffffffffu;
@@ -106,10 +114,11 @@ struct TopK {
 
 // Per-warp shared scratch: traversal stack, staged points, candidate buffers
 // ([slot][lane] so that a warp's accesses to one slot fall in distinct banks).
+template <int B>
 struct WarpSmem {
     int32_t stack[kStackDepth];
     float4 pts[kWindowMax];
-    int32_t buf[kBuf][32];
+    int32_t buf[B][32];
 };
 
 struct QArgs {
@@ -135,8 +144,8 @@ struct Counters {
 
 // Merge every lane's buffered candidates into its list; the warp steps
 // through max-over-lanes slots together.
-template <int K, bool EXACT>
-__device__ __forceinline__ void flush(TopK<K, EXACT>& tk, int& bc, WarpSmem& W, int lane, Counters& ct,
+template <int K, bool EXACT, class WS>
+__device__ __forceinline__ void flush(TopK<K, EXACT>& tk, int& bc, WS& W, int lane, Counters& ct,
                                       const float4* __restrict__ pts, float qx, float qy, float qz) {
     const int maxc = (int)__reduce_max_sync(FULL, (unsigned)bc);
     ct.merge += maxc;
@@ -158,9 +167,10 @@ __device__ __forceinline__ void flush(TopK<K, EXACT>& tk, int& bc, WarpSmem& W, 
 // Stage points [first, first + cnt) (cnt <= 32) in shared memory and append
 // every one whose distance reaches the lane's bound to the lane's buffer.
 // Points of the seed window [w0, w1) are skipped (they were already offered).
-// The caller guarantees bc + cnt <= kBuf.
+// The caller guarantees that bc + cnt fits the buffer.
+template <class WS>
 __device__ __forceinline__ void scan_chunk(int32_t first, int cnt, bool need, float qx, float qy, float qz,
-                                           float tau, int& bc, WarpSmem& W, const float4* __restrict__ pts,
+                                           float tau, int& bc, WS& W, const float4* __restrict__ pts,
                                            int32_t w0, int32_t w1, int lane) {
     if (lane < cnt) W.pts[lane] = __ldg(pts + first + lane);
     __syncwarp();
@@ -186,8 +196,9 @@ __device__ __forceinline__ void scan_chunk(int32_t first, int cnt, bool need, fl
 // one point of the bucket and the warp steps over the needing queries, so the
 // cost follows the number of needing lanes rather than the bucket size. Hits
 // are appended to the needing lane's buffer in ballot order.
+template <class WS>
 __device__ __forceinline__ void scan_sparse(int32_t first, int cnt, uint32_t mask, float qx, float qy, float qz,
-                                            float tau, int& bc, WarpSmem& W, const float4* __restrict__ pts,
+                                            float tau, int& bc, WS& W, const float4* __restrict__ pts,
                                             int32_t w0, int32_t w1, int lane) {
     const int32_t idx = first + lane;
     const bool has = lane < cnt && (idx < w0 || idx >= w1);
@@ -297,7 +308,8 @@ __device__ __forceinline__ void estimate_normal(const int32_t (&nbr)[K], int k, 
 template <int K, bool EXACT, bool EXT, bool NORMALS>
 __device__ __forceinline__ void knn_warp(const float4* __restrict__ pts, const SNode* __restrict__ snodes,
                                          const uint64_t* __restrict__ codes, const QArgs& a, DevState* st,
-                                         int64_t q0, WarpSmem& W, int lane) {
+                                         int64_t q0, WarpSmem<KnnCfg<K>::buf>& W, int lane) {
+    constexpr int kBuf = KnnCfg<K>::buf;
     const int64_t u = a.device_count ? (int64_t)st->u : a.u;
     const int64_t count = a.device_count ? u : a.count;
     if (q0 >= count) return;  // whole warp
@@ -508,11 +520,13 @@ __device__ __forceinline__ void knn_warp(const float4* __restrict__ pts, const S
 }
 
 template <int K, bool EXACT, bool EXT, bool NORMALS>
-__global__ void __launch_bounds__(kKnnThreads) k_knn(const float4* __restrict__ pts, const SNode* __restrict__ snodes,
+__global__ void __launch_bounds__(kKnnThreads, KnnCfg<K>::min_blocks)
+    k_knn(const float4* __restrict__ pts, const SNode* __restrict__ snodes,
                                                      const uint64_t* __restrict__ codes, QArgs a, DevState* st) {
     extern __shared__ __align__(16) unsigned char knn_smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    WarpSmem& W = reinterpret_cast<WarpSmem*>(knn_smem)[warp];
+    using WS = WarpSmem<KnnCfg<K>::buf>;
+    WS& W = reinterpret_cast<WS*>(knn_smem)[warp];
     const int64_t q0 = ((int64_t)blockIdx.x * kKnnWarps + warp) * 32;
     knn_warp<K, EXACT, EXT, NORMALS>(pts, snodes, codes, a, st, q0, W, lane);
 }
@@ -523,11 +537,13 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn(const float4* __restrict__ 
 // start first and the small ones fill the tail. Each cloud's size is read on
 // the device from its own build state.
 template <int K, bool EXACT>
-__global__ void __launch_bounds__(kKnnThreads) k_knn_batch(const BatchCloud* __restrict__ clouds, int n_clouds,
+__global__ void __launch_bounds__(kKnnThreads, KnnCfg<K>::min_blocks)
+    k_knn_batch(const BatchCloud* __restrict__ clouds, int n_clouds,
                                                            int64_t n_items, unsigned long long* counter, QArgs a) {
     extern __shared__ __align__(16) unsigned char knn_smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    WarpSmem& W = reinterpret_cast<WarpSmem*>(knn_smem)[warp];
+    using WS = WarpSmem<KnnCfg<K>::buf>;
+    WS& W = reinterpret_cast<WS*>(knn_smem)[warp];
     for (;;) {
         unsigned long long item = 0;
         if (lane == 0) item = atomicAdd(counter, 1ull);
@@ -551,7 +567,7 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn_batch(const BatchCloud* __r
 
 template <int K, bool EXACT, bool EXT, bool NORMALS>
 cudaError_t launch_one(const BuildBufs& b, const QArgs& a, unsigned blocks, cudaStream_t s) {
-    constexpr int smem = (int)sizeof(WarpSmem) * kKnnWarps;
+    constexpr int smem = (int)sizeof(WarpSmem<KnnCfg<K>::buf>) * kKnnWarps;
     cudaError_t e =
         cudaFuncSetAttribute(k_knn<K, EXACT, EXT, NORMALS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
@@ -571,7 +587,7 @@ cudaError_t launch_k(const BuildBufs& b, const QArgs& a, bool ext, bool normals,
 template <int K, bool EXACT>
 cudaError_t launch_batch(const BatchCloud* clouds, int n_clouds, int64_t n_items, unsigned long long* counter,
                          const QArgs& a, cudaStream_t s, int num_sms) {
-    constexpr int smem = (int)sizeof(WarpSmem) * kKnnWarps;
+    constexpr int smem = (int)sizeof(WarpSmem<KnnCfg<K>::buf>) * kKnnWarps;
     cudaError_t e = cudaFuncSetAttribute(k_knn_batch<K, EXACT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
