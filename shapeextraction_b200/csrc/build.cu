@@ -473,9 +473,15 @@ __global__ void k_root_parent(const int32_t* __restrict__ left_child, int32_t* _
 }
 
 // ---------------------------------------------------------------------------
-// Search boxes: bottom-up over the full-range radix tree (Karras 2012 sec. 4,
-// one thread per leaf, second arrival at a node merges). Writes each internal
-// node's SNode with both children's tight boxes and bucket references.
+// Search boxes: bottom-up over the full-range radix tree (Karras 2012 sec. 4:
+// second arrival at a node merges). Only nodes the kNN traversal visits need
+// an SNode: the root and every node of more than `bucket` points. A subtree
+// of at most `bucket` points is a bucket, read as a point range, so its inner
+// nodes get nothing: each leaf climbs to its bucket root (the highest
+// ancestor of at most `bucket` points) without atomics, the bucket's first
+// leaf scans the bucket's points for its box, and only that thread enters the
+// merge protocol at the bucket root's parent. A leaf whose parent is already
+// larger than a bucket is a bucket of one point.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_boxes(const float4* __restrict__ pts, const int32_t* __restrict__ left_child,
                                                const uint8_t* __restrict__ hll, const uint8_t* __restrict__ hlr,
@@ -487,9 +493,54 @@ __global__ void __launch_bounds__(256) k_boxes(const float4* __restrict__ pts, c
     const int64_t u = (int64_t)st->u;
     const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (p >= u || u < 2) return;
+    auto range_of = [&](int64_t c, int64_t& first, int64_t& last) {
+        const int64_t e = range_end[c];
+        first = min(c, e);
+        last = max(c, e);
+    };
+    // climb inside the bucket: c = bucket root (or the leaf itself), node = its parent
     int64_t node = leaf_parent[p];
+    int64_t c = -1;  // internal bucket root, or -1 when the leaf itself is the bucket
+    int64_t first = p, last = p;
+    for (int it = 0; it < 70; ++it) {
+        if (node < 0 || node >= u - 1) {
+            set_err(&st->err, ERRBIT_BOUNDS);
+            return;
+        }
+        if (node == 0) break;
+        int64_t f, l;
+        range_of(node, f, l);
+        if (l - f + 1 > bucket) break;
+        c = node;
+        first = f;
+        last = l;
+        node = sparent[node];
+        if (it == 69) {
+            set_err(&st->err, ERRBIT_BOUNDS);
+            return;
+        }
+    }
+    if (c >= 0) {
+        if (p != first) return;  // the bucket's first leaf carries it
+        float4 lo = __ldg(pts + first), hi = lo;
+        for (int64_t q = first + 1; q <= last; ++q) {
+            const float4 v = __ldg(pts + q);
+            lo.x = fminf(lo.x, v.x);
+            lo.y = fminf(lo.y, v.y);
+            lo.z = fminf(lo.z, v.z);
+            hi.x = fmaxf(hi.x, v.x);
+            hi.y = fmaxf(hi.y, v.y);
+            hi.z = fmaxf(hi.z, v.z);
+        }
+        node_box[2 * c] = make_float4(lo.x, lo.y, lo.z, 0.f);
+        node_box[2 * c + 1] = make_float4(hi.x, hi.y, hi.z, 0.f);
+    }
+    // merge protocol over the nodes the traversal visits
     for (int it = 0; it < 130; ++it) {
-        if (node < 0 || node >= u - 1) { set_err(&st->err, ERRBIT_BOUNDS); return; }
+        if (node < 0 || node >= u - 1) {
+            set_err(&st->err, ERRBIT_BOUNDS);
+            return;
+        }
         __threadfence();
         if (atomicAdd(&visit[node], 1u) == 0) return;
         __threadfence();
@@ -508,21 +559,21 @@ __global__ void __launch_bounds__(256) k_boxes(const float4* __restrict__ pts, c
         int32_t ref[2], cnt[2];
 #pragma unroll
         for (int side = 0; side < 2; ++side) {
-            const int64_t c = g + side;
+            const int64_t ch = g + side;
             const bool leaf = side ? r_leaf : l_leaf;
             if (leaf) {
-                const float4 q = pts[c];
+                const float4 q = pts[ch];
                 lo[side] = q;
                 hi[side] = q;
-                ref[side] = (int32_t)c;
+                ref[side] = (int32_t)ch;
                 cnt[side] = 1;
             } else {
-                lo[side] = __ldcg(node_box + 2 * c);
-                hi[side] = __ldcg(node_box + 2 * c + 1);
-                const int64_t e = range_end[c];
-                const int64_t first = min(c, e), last = max(c, e);
-                cnt[side] = (int32_t)(last - first + 1);
-                ref[side] = cnt[side] <= bucket ? (int32_t)first : (int32_t)c;
+                lo[side] = __ldcg(node_box + 2 * ch);
+                hi[side] = __ldcg(node_box + 2 * ch + 1);
+                int64_t f, l;
+                range_of(ch, f, l);
+                cnt[side] = (int32_t)(l - f + 1);
+                ref[side] = cnt[side] <= bucket ? (int32_t)f : (int32_t)ch;
             }
         }
         SNode sn;
