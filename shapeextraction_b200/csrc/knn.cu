@@ -62,6 +62,16 @@ __device__ __forceinline__ float key_d(unsigned long long k) { return __uint_as_
 // the new key with every entry independently and shifts in one step (no
 // serial chain). With EXACT = false the list is longer than k and the bound
 // is entry k-1.
+// key[i] for a run-time i, as a masked OR over all entries, so that the list
+// stays in registers (a direct key[i] would move it to local memory).
+template <int K>
+__device__ __forceinline__ unsigned long long pick(const unsigned long long (&key)[K], int i) {
+    unsigned long long acc = 0;
+#pragma unroll
+    for (int j = 0; j < K; ++j) acc |= key[j] & (0ull - (unsigned long long)(j == i));
+    return acc;
+}
+
 template <int K, bool EXACT>
 struct TopK {
     unsigned long long key[K];
@@ -90,9 +100,7 @@ struct TopK {
         if (EXACT) {
             bk = key[K - 1];
         } else {
-#pragma unroll
-            for (int j = 0; j < K; ++j)
-                if (j == kk - 1) bk = key[j];
+            bk = pick(key, kk - 1);
         }
     }
     __device__ __forceinline__ void insert(unsigned long long nk) {  // requires nk < bk
@@ -105,9 +113,7 @@ struct TopK {
         if (EXACT) {
             bk = key[K - 1];
         } else {
-#pragma unroll
-            for (int j = 0; j < K; ++j)
-                if (j == kk - 1) bk = key[j];
+            bk = pick(key, kk - 1);
         }
     }
 };
