@@ -74,6 +74,7 @@ __device__ __forceinline__ unsigned long long pick(const unsigned long long (&ke
 
 template <int K, bool EXACT>
 struct TopK {
+    static_assert(K % 2 == 0, "list sizes are even");
     unsigned long long key[K];
     unsigned long long bk;  // entry k-1: the pruning bound
     int kk;
@@ -88,10 +89,19 @@ struct TopK {
     // odd-even transposition network (K passes of independent
     // compare-exchanges) and set the bound.
     __device__ __forceinline__ void sort_filled() {
+        // K passes as K/2 rolled (even, odd) pairs: the same exchanges as a
+        // fully unrolled network in K instead of K*K/2 instructions' worth of
+        // code, which keeps large-k kernels inside the instruction cache
+#pragma unroll 1
+        for (int pass = 0; pass < K; pass += 2) {
 #pragma unroll
-        for (int pass = 0; pass < K; ++pass) {
+            for (int j = 0; j + 1 < K; j += 2) {
+                const unsigned long long a = key[j], b = key[j + 1];
+                key[j] = a < b ? a : b;
+                key[j + 1] = a < b ? b : a;
+            }
 #pragma unroll
-            for (int j = pass & 1; j + 1 < K; j += 2) {
+            for (int j = 1; j + 1 < K; j += 2) {
                 const unsigned long long a = key[j], b = key[j + 1];
                 key[j] = a < b ? a : b;
                 key[j + 1] = a < b ? b : a;
