@@ -240,19 +240,19 @@ __device__ __forceinline__ void neu_add(float& s, float& c, float x) {
     s = t;
 }
 
-// Normal of one query from its k neighbours (nbr[0..k), ascending):
+// Normal of one query from its k neighbours, ascending, whose indices are in
+// nbr[0], nbr[32], ... (the lane's column of the candidate buffer, free once
+// the search is done; rolled loops keep the code small for large k):
 // centred covariance with compensated FP32 sums, FP32 Jacobi, FP64 redo when
 // the relative eigengap (l1 - l0) / l2 is below `gap`, orientation towards
 // the viewpoint (src/NormalEstimation.hpp:184-189).
-template <int K>
-__device__ __forceinline__ void estimate_normal(const int32_t (&nbr)[K], int k, const float4* __restrict__ pts,
+__device__ __forceinline__ void estimate_normal(const int32_t* nbr, int k, const float4* __restrict__ pts,
                                                 float qx, float qy, float qz, const QArgs& a, float* out,
                                                 DevState* st) {
     float s[3] = {0.f, 0.f, 0.f}, c[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-    for (int j = 0; j < K; ++j) {
-        if (j >= k) break;
-        const float4 p = __ldg(pts + nbr[j]);
+#pragma unroll 4
+    for (int j = 0; j < k; ++j) {
+        const float4 p = __ldg(pts + nbr[32 * j]);
         neu_add(s[0], c[0], p.x - qx);
         neu_add(s[1], c[1], p.y - qy);
         neu_add(s[2], c[2], p.z - qz);
@@ -260,10 +260,9 @@ __device__ __forceinline__ void estimate_normal(const int32_t (&nbr)[K], int k, 
     const float inv_k = 1.0f / (float)k;
     const float m0 = (s[0] + c[0]) * inv_k, m1 = (s[1] + c[1]) * inv_k, m2 = (s[2] + c[2]) * inv_k;
     float cs[6] = {0, 0, 0, 0, 0, 0}, cc[6] = {0, 0, 0, 0, 0, 0};
-#pragma unroll
-    for (int j = 0; j < K; ++j) {
-        if (j >= k) break;
-        const float4 p = __ldg(pts + nbr[j]);
+#pragma unroll 4
+    for (int j = 0; j < k; ++j) {
+        const float4 p = __ldg(pts + nbr[32 * j]);
         const float r0 = (p.x - qx) - m0, r1 = (p.y - qy) - m1, r2 = (p.z - qz) - m2;
         neu_add(cs[0], cc[0], r0 * r0);
         neu_add(cs[1], cc[1], r0 * r1);
@@ -283,20 +282,18 @@ __device__ __forceinline__ void estimate_normal(const int32_t (&nbr)[K], int k, 
     if (!(gap >= a.gap)) {
         // near-degenerate neighbourhood: redo covariance and eigensolve in FP64
         double sd[3] = {0, 0, 0};
-#pragma unroll
-        for (int j = 0; j < K; ++j) {
-            if (j >= k) break;
-            const float4 p = __ldg(pts + nbr[j]);
+#pragma unroll 1
+        for (int j = 0; j < k; ++j) {
+            const float4 p = __ldg(pts + nbr[32 * j]);
             sd[0] += (double)p.x - (double)qx;
             sd[1] += (double)p.y - (double)qy;
             sd[2] += (double)p.z - (double)qz;
         }
         const double md[3] = {sd[0] / k, sd[1] / k, sd[2] / k};
         double Cd[6] = {0, 0, 0, 0, 0, 0};
-#pragma unroll
-        for (int j = 0; j < K; ++j) {
-            if (j >= k) break;
-            const float4 p = __ldg(pts + nbr[j]);
+#pragma unroll 1
+        for (int j = 0; j < k; ++j) {
+            const float4 p = __ldg(pts + nbr[32 * j]);
             const double r0 = ((double)p.x - (double)qx) - md[0];
             const double r1 = ((double)p.y - (double)qy) - md[1];
             const double r2 = ((double)p.z - (double)qz) - md[2];
@@ -326,6 +323,7 @@ __device__ __forceinline__ void knn_warp(const float4* __restrict__ pts, const S
                                          const uint64_t* __restrict__ codes, const QArgs& a, DevState* st,
                                          int64_t q0, WarpSmem<KnnCfg<K>::buf>& W, int lane) {
     constexpr int kBuf = KnnCfg<K>::buf;
+    static_assert(K <= kBuf, "the neighbour list is staged in the candidate buffer");
     const int64_t u = a.device_count ? (int64_t)st->u : a.u;
     const int64_t count = a.device_count ? u : a.count;
     if (q0 >= count) return;  // whole warp
@@ -532,7 +530,11 @@ __device__ __forceinline__ void knn_warp(const float4* __restrict__ pts, const S
         for (int j = 0; j < K; ++j)
             if (j < a.k) o[j] = key_d(tk.key[j]);
     }
-    if (NORMALS) estimate_normal<K>(nbr, a.k, pts, qx, qy, qz, a, a.out_normals + 3 * qo, st);
+    if (NORMALS) {
+#pragma unroll
+        for (int j = 0; j < K; ++j) W.buf[j][lane] = nbr[j];  // this lane's column only
+        estimate_normal(&W.buf[0][lane], a.k, pts, qx, qy, qz, a, a.out_normals + 3 * qo, st);
+    }
 }
 
 template <int K, bool EXACT, bool EXT, bool NORMALS>
