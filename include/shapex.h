@@ -56,7 +56,9 @@ typedef struct se_options {
     int32_t seed_halo;     /* kNN: points offered on each side of a warp's 32 queries
                               before the tree walk (0..48; -1 = default) */
     int32_t learned;       /* 1: queries start from the learned radius (se_mlp_*);
-                              queries it underestimates are searched again without it */
+                              queries it underestimates are searched again without it.
+                              Applies to the tree's own points (se_knn_self,
+                              se_normals), not to se_knn or se_normals_batch */
     int32_t learned_skip_seed; /* with learned: skip the Morton-window seed */
     int32_t search_compat; /* 1: se_knn, se_knn_self and se_normals run the reference's
                               own approximate search (knnSearchKernel<k>,

@@ -403,20 +403,23 @@ __device__ __forceinline__ void knn_warp(const float4* __restrict__ pts, const S
                 }
                 tk.sort_filled();
             }
+            // the rest of the window in runs of at most kBuf steps (a step
+            // buffers at most one point per lane), one merge after each run
             float tau = fminf(tk.tau(), cap);
-            for (int t = K; t < nsteps; ++t) {
-                const int off = (t & 1) ? (t + 1) >> 1 : -(t >> 1);
-                const int iw = p + off;
-                if (act && iw >= 0 && iw < S) {
-                    const float4 q = W.pts[iw];
-                    if (dist2(qx, qy, qz, q.x, q.y, q.z) <= tau) W.buf[bc++][lane] = (int32_t)(w0 + iw);
+            int t = K;
+            do {
+                const int lim = min(nsteps, t + kBuf);
+                for (; t < lim; ++t) {
+                    const int off = (t & 1) ? (t + 1) >> 1 : -(t >> 1);
+                    const int iw = p + off;
+                    if (act && iw >= 0 && iw < S) {
+                        const float4 q = W.pts[iw];
+                        if (dist2(qx, qy, qz, q.x, q.y, q.z) <= tau) W.buf[bc++][lane] = (int32_t)(w0 + iw);
+                    }
                 }
-                if (__any_sync(FULL, bc == kBuf)) {
-                    flush(tk, bc, W, lane, ct, pts, qx, qy, qz);
-                    tau = fminf(tk.tau(), cap);
-                }
-            }
-            flush(tk, bc, W, lane, ct, pts, qx, qy, qz);
+                flush(tk, bc, W, lane, ct, pts, qx, qy, qz);
+                tau = fminf(tk.tau(), cap);
+            } while (t < nsteps);
         }
 
         if (u >= 2 && (sw0 > 0 || sw1 < u)) {
