@@ -20,8 +20,8 @@ CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 BUILD_DIR = os.path.join(ROOT, "_build")
 LIB = os.path.join(PKG, "libshapex.so")
-SOURCES = ["capi.cu", "build.cu", "knn.cu", "mlp.cu", "static_sort.cu", "compat.cu"]
-HEADERS = ["common.cuh", "pipeline.cuh", "eig3.cuh"]
+SOURCES = ["capi.cu", "capi_mlp.cu", "capi_batch.cu", "build.cu", "knn.cu", "mlp.cu", "static_sort.cu", "compat.cu"]
+HEADERS = ["common.cuh", "pipeline.cuh", "eig3.cuh", "context.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
