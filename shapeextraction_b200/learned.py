@@ -43,9 +43,13 @@ def _sample(ctx: Context, k: int, max_rows: int, rng) -> tuple[np.ndarray, np.nd
 
 
 def train_radius_model(ctx: Context, k: int, steps: int = 1500, batch: int = 8192, lr: float = 2e-3, seed: int = 0,
-                       quantile: float = 0.99, max_rows: int = 1_000_000) -> dict:
+                       quantile: float = 0.995, max_rows: int = 1_000_000) -> dict:
     """Train the context's model on its own built cloud (the held-out cloud)
-    and calibrate the margin. Returns the losses and the calibration."""
+    and calibrate the margin at the `quantile` of the training residuals.
+    A warp searches again whenever one of its 32 lanes misses, so misses cost
+    far more than a slightly looser bound: 0.995 measured best on surface,
+    mixture and precision-mix clouds (0.99 and 0.999 were 1-4% slower).
+    Returns the losses and the calibration."""
     rng = np.random.default_rng(seed)
     X, y = _sample(ctx, k, max_rows, rng)
     perm = rng.permutation(y.size)
