@@ -23,6 +23,14 @@ extern "C" {
 
 #define SE_ABI_VERSION 1
 
+/* The library exports exactly the functions below; everything else in it is
+ * hidden. */
+#if defined(__GNUC__)
+#define SE_API __attribute__((visibility("default")))
+#else
+#define SE_API
+#endif
+
 typedef enum se_status {
     SE_OK = 0,
     SE_ERR_INVALID_ARG = 1,   /* bad pointer, size, k or option */
@@ -110,15 +118,15 @@ typedef struct se_device_views {
     const uint8_t* has_leaf_right;
 } se_device_views;
 
-int se_options_init(se_options* opt);
-const char* se_status_string(int status);
-int se_abi_version(void);
+SE_API int se_options_init(se_options* opt);
+SE_API const char* se_status_string(int status);
+SE_API int se_abi_version(void);
 
 /* Context lifetime. Replaces the implicit global state of the reference
  * (default stream, per-call cudaMallocManaged). */
-int se_create(se_ctx** ctx, const se_options* opt);
-int se_destroy(se_ctx* ctx);
-const char* se_last_error(const se_ctx* ctx);
+SE_API int se_create(se_ctx** ctx, const se_options* opt);
+SE_API int se_destroy(se_ctx* ctx);
+SE_API const char* se_last_error(const se_ctx* ctx);
 
 /* Replaces RT::RadixTree::RadixTree(const PointCloud<float>&)
  * (src/RadixTree.hpp:38, src/RadixTree.cu:305-382) followed by
@@ -126,43 +134,43 @@ const char* se_last_error(const se_ctx* ctx);
  * src/Octree.cu:213-319): bbox, Morton encode, sort, dedup, Karras radix tree,
  * octree, decode. x, y, z are the SoA coordinate arrays of PointCloud<float>
  * (src/PointCloud.hpp:105-122). Returns after the build has finished. */
-int se_build(se_ctx* ctx, const float* x, const float* y, const float* z, int64_t n, int mem);
+SE_API int se_build(se_ctx* ctx, const float* x, const float* y, const float* z, int64_t n, int mem);
 
 /* RadixTree::n_pts/n_nodes/min_coord/max_coord, Octree::n_pts/n_nodes. */
-int se_get_info(const se_ctx* ctx, se_info* info);
+SE_API int se_get_info(const se_ctx* ctx, se_info* info);
 /* Device pointers to the built arrays (RadixTree::d_tree, Octree::u_nodes, Octree::u_points). */
-int se_get_device_views(const se_ctx* ctx, se_device_views* views);
+SE_API int se_get_device_views(const se_ctx* ctx, se_device_views* views);
 
 /* Copies of the build stages for parity checks. */
 /* RT::Nodes::mortonCode after dedup (src/RadixTree.cu:294-296): u codes, ascending. */
-int se_get_codes(se_ctx* ctx, uint64_t* out, int mem);
+SE_API int se_get_codes(se_ctx* ctx, uint64_t* out, int mem);
 /* RT::Nodes arrays, src/RadixTree.cu:344-362: n_radix entries each; parent has
  * u entries (entries never written by the tree, e.g. parent[0], are 0). */
-int se_get_radix(se_ctx* ctx, int32_t* left_child, int32_t* parent, uint8_t* prefix_n,
+SE_API int se_get_radix(se_ctx* ctx, int32_t* left_child, int32_t* parent, uint8_t* prefix_n,
                  uint8_t* has_leaf_left, uint8_t* has_leaf_right, int mem);
 /* Octree::u_nodes, src/Octree.cu:250-282: n_octree nodes. */
-int se_get_octree(se_ctx* ctx, se_otnode* out, int mem);
+SE_API int se_get_octree(se_ctx* ctx, se_otnode* out, int mem);
 /* Octree::u_points / h_points, src/Octree.cu:305-318: u points, AoS xyz. */
-int se_get_points(se_ctx* ctx, float* out_xyz, int mem);
+SE_API int se_get_points(se_ctx* ctx, float* out_xyz, int mem);
 
 /* Replaces Octree::deviceKnnSearch<k>(d_query, d_nn, N, eps) (src/Octree.hpp:106-107,
  * 199-212) with the tree's own points [start, start+count) as queries, as
  * NormalEstimation::estimateNormals does (src/NormalEstimation.hpp:204,211).
  * Exact kNN, rows ascending by (squared distance, index); out_idx count*k
  * int32, out_d2 (optional, may be NULL) count*k float. 1 <= k <= 32. */
-int se_knn_self(se_ctx* ctx, int k, int64_t start, int64_t count, int32_t* out_idx, float* out_d2, int mem);
+SE_API int se_knn_self(se_ctx* ctx, int k, int64_t start, int64_t count, int32_t* out_idx, float* out_d2, int mem);
 
 /* Replaces Octree::knnSearch<k>(points, eps) (src/Octree.hpp:102-103, 214-242)
  * for arbitrary query points (AoS xyz, n_queries of them), with the
  * reference's N/eps argument swap (src/Octree.hpp:232) not reproduced. */
-int se_knn(se_ctx* ctx, int k, const float* queries_xyz, int64_t n_queries, int32_t* out_idx, float* out_d2,
+SE_API int se_knn(se_ctx* ctx, int k, const float* queries_xyz, int64_t n_queries, int32_t* out_idx, float* out_d2,
            int mem);
 
 /* Replaces NormalEstimation::estimateNormals<k>(octree, start_idx, n)
  * (src/NormalEstimation.hpp:16-19, 196-335): exact kNN, covariance, 3x3
  * symmetric eigensolve, orientation towards the viewpoint, fused in one
  * kernel. out_xyz: count normals, AoS xyz (std::vector<Point> layout). */
-int se_normals(se_ctx* ctx, int k, int64_t start, int64_t count, float* out_xyz, int mem);
+SE_API int se_normals(se_ctx* ctx, int k, int64_t start, int64_t count, float* out_xyz, int mem);
 
 /* Batched normal estimation over n_clouds independent clouds; no counterpart
  * in the reference (one cloud per call there). The clouds are concatenated
@@ -178,7 +186,7 @@ int se_normals(se_ctx* ctx, int k, int64_t start, int64_t count, float* out_xyz,
  * offsets[n_clouds] rows of xyz: cloud c's u_c normals (its unique points in
  * Morton order) start at row offsets[c]; out_u[c] = u_c. offsets, ks and out_u
  * are host arrays; x, y, z and out_normals follow `mem`. */
-int se_normals_batch(se_ctx* ctx, const float* x, const float* y, const float* z, const int64_t* offsets,
+SE_API int se_normals_batch(se_ctx* ctx, const float* x, const float* y, const float* z, const int64_t* offsets,
                      int n_clouds, const int32_t* ks, float* out_normals, int64_t* out_u, int mem);
 
 /* Work counters of the last se_normals/se_knn/se_knn_self call (diagnostics). */
@@ -191,7 +199,7 @@ typedef struct se_stats {
     int64_t inserts;         /* insertions into the k-best lists, summed over queries */
     int64_t learned_misses;  /* queries whose learned radius was too small (searched again) */
 } se_stats;
-int se_get_stats(const se_ctx* ctx, se_stats* stats);
+SE_API int se_get_stats(const se_ctx* ctx, se_stats* stats);
 
 /* Device timings of the last se_build and query call, from CUDA events
  * recorded on the context's stream around each stage, and the number of
@@ -203,7 +211,7 @@ typedef struct se_profile {
     int32_t build_launches;
     int32_t query_launches;
 } se_profile;
-int se_get_profile(se_ctx* ctx, se_profile* prof);
+SE_API int se_get_profile(se_ctx* ctx, se_profile* prof);
 
 /* ---- Learned search radius. No counterpart in the reference (the north
  * star's learned stage): a 32 -> 64 -> 64 -> 1 MLP with BF16 weights and FP32
@@ -214,31 +222,31 @@ int se_get_profile(se_ctx* ctx, se_profile* prof);
 #define SE_MLP_FEATURES 32
 #define SE_MLP_PARAMS 6337
 /* Features of tree points [start, start+count): count x SE_MLP_FEATURES floats. */
-int se_features(se_ctx* ctx, int64_t start, int64_t count, float* out, int mem);
+SE_API int se_features(se_ctx* ctx, int64_t start, int64_t count, float* out, int mem);
 /* Random initialisation (uniform He scaling), biases zero. */
-int se_mlp_init(se_ctx* ctx, uint64_t seed);
+SE_API int se_mlp_init(se_ctx* ctx, uint64_t seed);
 /* Copy the FP32 master parameters out (set = 0) or in (set = 1). */
-int se_mlp_params(se_ctx* ctx, float* params, int set, int mem);
+SE_API int se_mlp_params(se_ctx* ctx, float* params, int set, int mem);
 /* Turn the learned starting bound on/off for later queries (se_options.learned
  * and .learned_skip_seed at run time). */
-int se_mlp_enable(se_ctx* ctx, int learned, int skip_seed);
+SE_API int se_mlp_enable(se_ctx* ctx, int learned, int skip_seed);
 /* Log-margin added to predictions to make them upper bounds. */
-int se_mlp_set_margin(se_ctx* ctx, float margin_log2);
+SE_API int se_mlp_set_margin(se_ctx* ctx, float margin_log2);
 /* Forward pass of the training path (CUDA cores): out[n] = y-hat. */
-int se_mlp_forward(se_ctx* ctx, const float* features, int64_t n, float* out, int mem);
+SE_API int se_mlp_forward(se_ctx* ctx, const float* features, int64_t n, float* out, int mem);
 /* Tensor-core inference fused with the features, on tree points
  * [start, start+count): y-hat and/or the search bound r^2 (either may be NULL). */
-int se_mlp_predict(se_ctx* ctx, int64_t start, int64_t count, float* yhat, float* r2, int mem);
+SE_API int se_mlp_predict(se_ctx* ctx, int64_t start, int64_t count, float* yhat, float* r2, int mem);
 /* Mean squared error and its gradient w.r.t. every parameter (SE_MLP_PARAMS floats). */
-int se_mlp_grad(se_ctx* ctx, const float* features, const float* targets, int64_t n, float* grads, float* loss,
+SE_API int se_mlp_grad(se_ctx* ctx, const float* features, const float* targets, int64_t n, float* grads, float* loss,
                 int mem);
 /* Adam on the MSE over `steps` consecutive mini-batches of `batch` rows
  * (cycling over the n rows); losses (optional, `steps` floats) per step. */
-int se_mlp_train(se_ctx* ctx, const float* features, const float* targets, int64_t n, int steps, int batch, float lr,
+SE_API int se_mlp_train(se_ctx* ctx, const float* features, const float* targets, int64_t n, int steps, int batch, float lr,
                  float* losses, int mem);
 /* Parameters + margin to / from a file (magic "SXMLP1", F, H, params, margin). */
-int se_mlp_save(se_ctx* ctx, const char* path);
-int se_mlp_load(se_ctx* ctx, const char* path);
+SE_API int se_mlp_save(se_ctx* ctx, const char* path);
+SE_API int se_mlp_load(se_ctx* ctx, const char* path);
 
 /* Sorts n 64-bit keys (e.g. Morton codes) ascending on the current device
  * WITHOUT ALLOCATING. It has no counterpart in the reference.
@@ -259,10 +267,10 @@ int se_mlp_load(se_ctx* ctx, const char* path);
  *   returns after the sort has finished. */
 #define SE_STATIC_SORT_MAX_KEYS (1 << 20)
 #define SE_STATIC_SORT_BYTES (8u * (1u << 20) + 256u * 1024u + 20480u)
-int se_sort_keys_static(const uint64_t* d_keys_in, uint64_t* d_keys_out, int64_t n, void* stream);
+SE_API int se_sort_keys_static(const uint64_t* d_keys_in, uint64_t* d_keys_out, int64_t n, void* stream);
 
 /* Waits for all work queued on the context's stream. */
-int se_synchronize(se_ctx* ctx);
+SE_API int se_synchronize(se_ctx* ctx);
 
 #ifdef __cplusplus
 }

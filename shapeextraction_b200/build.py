@@ -37,7 +37,7 @@ def _host_cc():
 
 
 def _flags(ptxas_v):
-    f = ["-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC,-O2", "-ccbin", _host_cc(), "-I", INCLUDE,
+    f = ["-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC,-O2,-fvisibility=hidden", "-ccbin", _host_cc(), "-I", INCLUDE,
          "-I", CSRC]
     if ptxas_v:
         f += ["-Xptxas", "-v"]

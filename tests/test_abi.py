@@ -62,3 +62,18 @@ def test_create_without_gpu_fails_cleanly(native):
         pytest.skip("a GPU is present")
     with pytest.raises(native.ShapexError):
         native.Context()
+
+
+def test_library_exports_only_the_c_abi(native):
+    """Internal C++ helpers stay hidden; the exported se_ symbols are exactly
+    the declared entry points."""
+    import shutil
+    import subprocess
+
+    nm = shutil.which("nm")
+    if nm is None:
+        pytest.skip("nm not available")
+    out = subprocess.run([nm, "-D", "--defined-only", native.LIB_PATH], capture_output=True, text=True, check=True)
+    names = [ln.split()[-1] for ln in out.stdout.splitlines() if ln.strip()]
+    assert sorted(n for n in names if n.startswith("se_")) == header_functions()
+    assert not [n for n in names if "shapex" in n]
