@@ -137,7 +137,7 @@ def test_knn_external_queries(native, oracle):
         assert np.array_equal(idx, ei)
 
 
-@pytest.mark.parametrize("k", [8, 16, 32])
+@pytest.mark.parametrize("k", [8, 12, 16, 24, 32])
 def test_normals_vs_fp64_oracle(native, oracle, k):
     x, y, z = synth.scene(60000, 31)
     with _ctx(native) as c:
