@@ -299,7 +299,8 @@ def run_ours(a):
                        "k": k, "code_bits": wl["code_bits"], "octree_nodes": int(m),
                        "l2": "flushed by a 256 MB device write before every timed step",
                        "parallelism": f"{world} independent replica(s), one cloud per GPU",
-                       "leaf_bucket": a.bucket, "seed_halo": a.halo, "eigengap_fp64": a.eigengap},
+                       "leaf_bucket": a.bucket, "seed_halo": a.halo if a.halo >= 0 else (32 if k > 16 else 16),
+                       "eigengap_fp64": a.eigengap},
             "e2e": {"value": u_all * a.steps / (ms_e2e * 1e-3), "unit": "normals/s",
                     "ms_per_step": ms_e2e / a.steps, "h2d_bytes_per_step": int(12 * n),
                     "d2h_bytes_per_step": int(12 * u)},
@@ -423,7 +424,8 @@ def run_batch(a):
             "pipeline": "plain (batched)",
             "config": {"workload": a.workload, "desc": wl["desc"], "clouds": len(clouds), "n_points": total,
                        "unique_points": u_sum, "k_counts": {str(k): int((ks == k).sum()) for k in (8, 16, 32)},
-                       "leaf_bucket": bucket, "seed_halo": halo, "autotune": tuning,
+                       "leaf_bucket": bucket,
+                       "seed_halo": halo if halo >= 0 else "per k: 16 up to k=16, 32 above", "autotune": tuning,
                        "l2": "flushed by a 256 MB device write before every timed step",
                        "parallelism": f"{world} independent replica(s), one batch per GPU"},
             "e2e": {"value": u_all * a.steps / (ms_e2e * 1e-3), "unit": "normals/s", "ms_per_step": ms_e2e / a.steps,
@@ -585,7 +587,8 @@ def main():
     ap.add_argument("--workload", default="scene_2M_k16")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--bucket", type=int, default=32)
-    ap.add_argument("--halo", type=int, default=16)
+    ap.add_argument("--halo", type=int, default=-1,
+                    help="seed halo (-1: the library's per-k default, 16 up to k=16 and 32 above)")
     ap.add_argument("--eigengap", type=float, default=None,
                     help="FP64-redo eigengap threshold (default: the workload's, else 1e-4)")
     ap.add_argument("--cpu-sample", type=int, default=200_000)

@@ -62,7 +62,8 @@ typedef struct se_options {
     int32_t device;        /* CUDA device ordinal */
     void* stream;          /* cudaStream_t to use; NULL: the context creates one */
     int32_t seed_halo;     /* kNN: points offered on each side of a warp's 32 queries
-                              before the tree walk (0..48; -1 = default) */
+                              before the tree walk (0..48); -1 (the default) picks
+                              per k: 16 up to k = 16, 32 above (measured best) */
     int32_t learned;       /* 1: queries start from the learned radius (se_mlp_*);
                               queries it underestimates are searched again without it.
                               Applies to the tree's own points (se_knn_self,

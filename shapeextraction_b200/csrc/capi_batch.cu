@@ -146,7 +146,7 @@ int enqueue_batch(se_ctx* c, const BatchPlan& plan, const BatchCloud* d_desc, co
                 q.eigengap_fp64 = c->opt.eigengap_fp64;
                 q.code_bits = c->opt.code_bits;
                 q.bucket = c->opt.leaf_bucket;
-                q.seed_halo = c->opt.seed_halo;
+                q.seed_halo = seed_halo_for(c, q.k);
                 SE_CUDA(c, enqueue_query(b, q, lane.stream, c->num_sms), "launch batch query");
                 ++launches;
             }
@@ -165,7 +165,7 @@ int enqueue_batch(se_ctx* c, const BatchPlan& plan, const BatchCloud* d_desc, co
         q.eigengap_fp64 = c->opt.eigengap_fp64;
         q.code_bits = c->opt.code_bits;
         q.bucket = c->opt.leaf_bucket;
-        q.seed_halo = c->opt.seed_halo;
+        q.seed_halo = seed_halo_for(c, q.k);
         const int first = plan.group_first[gi], count = plan.group_first[gi + 1] - first;
         SE_CUDA(c, enqueue_query_batch(d_desc + first, count, plan.group_items[gi], c->batch_counter + gi, q, g,
                                        c->num_sms),

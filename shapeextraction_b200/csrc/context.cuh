@@ -122,6 +122,8 @@ int check_err_bits(se_ctx* c, uint32_t err);
 // Makes the context's device current.
 int prologue(se_ctx* c);
 int check_mem(se_ctx* c, int mem);
+// The seed halo a query of k neighbours uses (the option, or its per-k default).
+int seed_halo_for(const se_ctx* c, int k);
 
 #define SE_CUDA(c, call, where)                                          \
     do {                                                                 \
