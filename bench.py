@@ -586,7 +586,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="scene_2M_k16")
     ap.add_argument("--seed", type=int, default=1)
-    ap.add_argument("--bucket", type=int, default=32)
+    ap.add_argument("--bucket", type=int, default=96)
     ap.add_argument("--halo", type=int, default=-1,
                     help="seed halo (-1: the library's per-k default, 16 up to k=16 and 32 above)")
     ap.add_argument("--eigengap", type=float, default=None,

@@ -58,7 +58,8 @@ typedef struct se_options {
     float eigengap_fp64;   /* relative eigengap (l1-l0)/l2 below which the 3x3
                               eigensolve is redone in FP64 on the GPU */
     int32_t leaf_bucket;   /* kNN bucket size: subtrees of <= this many points are
-                              scanned directly (1..32; 0 = default) */
+                              scanned directly, 32 at a time (1..128; 0 or the
+                              default: 96) */
     int32_t device;        /* CUDA device ordinal */
     void* stream;          /* cudaStream_t to use; NULL: the context creates one */
     int32_t seed_halo;     /* kNN: points offered on each side of a warp's 32 queries

@@ -161,7 +161,7 @@ class Context:
     """One se_ctx: device memory and a CUDA stream for one host thread."""
 
     def __init__(self, code_bits=63, root_compat=True, build_octree=True, viewpoint=(0.0, 0.0, 0.0),
-                 eigengap_fp64=1e-4, leaf_bucket=32, device=0, stream=None, seed_halo=-1, learned=False,
+                 eigengap_fp64=1e-4, leaf_bucket=96, device=0, stream=None, seed_halo=-1, learned=False,
                  learned_skip_seed=False, search_compat=False, batch_graph=True):
         L = lib()
         o = SeOptions()

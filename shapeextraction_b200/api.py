@@ -62,7 +62,7 @@ class RadixTree:
     unless build_octree=False, the octree) in one call."""
 
     def __init__(self, cloud: PointCloud, code_bits=63, root_compat=True, build_octree=True, viewpoint=(0, 0, 0),
-                 eigengap_fp64=1e-4, leaf_bucket=32, device=0, context: Context | None = None):
+                 eigengap_fp64=1e-4, leaf_bucket=96, device=0, context: Context | None = None):
         self.ctx = context or Context(code_bits=code_bits, root_compat=root_compat, build_octree=build_octree,
                                       viewpoint=viewpoint, eigengap_fp64=eigengap_fp64, leaf_bucket=leaf_bucket,
                                       device=device)

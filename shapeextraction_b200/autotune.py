@@ -19,7 +19,7 @@ import numpy as np
 
 from ._native import Context
 
-CANDIDATES = [(b, h) for b in (16, 24, 32) for h in (8, 16, 32)]
+CANDIDATES = [(b, h) for b in (32, 64, 96) for h in (8, 16, 32)]
 DEFAULT_CACHE = os.path.join(os.path.expanduser("~"), ".cache", "shapeextraction_b200", "autotune.json")
 
 

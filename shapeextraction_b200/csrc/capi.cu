@@ -273,7 +273,7 @@ int se_options_init(se_options* o) {
     o->build_octree = 1;
     o->viewpoint[0] = o->viewpoint[1] = o->viewpoint[2] = 0.0f;
     o->eigengap_fp64 = 1e-4f;
-    o->leaf_bucket = 32;
+    o->leaf_bucket = 96;
     o->device = 0;
     o->stream = nullptr;
     o->seed_halo = -1;
@@ -306,8 +306,8 @@ int se_create(se_ctx** out, const se_options* opt) {
     se_options o;
     if (opt) o = *opt; else se_options_init(&o);
     if (o.code_bits != 63 && o.code_bits != 30) return SE_ERR_INVALID_ARG;
-    if (o.leaf_bucket == 0) o.leaf_bucket = 32;
-    if (o.leaf_bucket < 1 || o.leaf_bucket > 32) return SE_ERR_INVALID_ARG;
+    if (o.leaf_bucket == 0) o.leaf_bucket = 96;
+    if (o.leaf_bucket < 1 || o.leaf_bucket > 128) return SE_ERR_INVALID_ARG;
     if (o.seed_halo < 0) o.seed_halo = -1;  // per-k default, resolved by seed_halo_for
     if (o.seed_halo > 48) return SE_ERR_INVALID_ARG;
     if (!(o.eigengap_fp64 >= 0.0f)) return SE_ERR_INVALID_ARG;

@@ -492,13 +492,19 @@ __device__ __forceinline__ void knn_warp(const float4* __restrict__ pts, const S
                     const bool need = act && (left ? dl : dr) <= bnd;
                     const uint32_t needm = __ballot_sync(FULL, need);
                     if (!needm) continue;
-                    if (__any_sync(FULL, bc + cnt > kBuf)) flush(tk, bc, W, lane, ct, pts, qx, qy, qz);
                     ++ct.buckets;
-                    const float b2 = fminf(tk.tau(), cap);
-                    if (3 * __popc(needm) < 2 * cnt)
-                        scan_sparse(first, cnt, needm, qx, qy, qz, b2, bc, W, pts, (int32_t)sw0, (int32_t)sw1, lane);
-                    else
-                        scan_chunk(first, cnt, need, qx, qy, qz, b2, bc, W, pts, (int32_t)sw0, (int32_t)sw1, lane);
+                    // buckets of more than 32 points go in 32-point chunks
+                    for (int c0 = 0; c0 < cnt; c0 += 32) {
+                        const int32_t f = first + c0;
+                        const int n = min(32, cnt - c0);
+                        if (f >= sw0 && f + n <= sw1) continue;  // this chunk was in the seed window
+                        if (__any_sync(FULL, bc + n > kBuf)) flush(tk, bc, W, lane, ct, pts, qx, qy, qz);
+                        const float b2 = fminf(tk.tau(), cap);
+                        if (3 * __popc(needm) < 2 * n)
+                            scan_sparse(f, n, needm, qx, qy, qz, b2, bc, W, pts, (int32_t)sw0, (int32_t)sw1, lane);
+                        else
+                            scan_chunk(f, n, need, qx, qy, qz, b2, bc, W, pts, (int32_t)sw0, (int32_t)sw1, lane);
+                    }
                 }
 #pragma unroll
                 for (int o = 1; o >= 0; --o) {

@@ -102,7 +102,7 @@ def test_knn_exact_bit_exact(native, oracle, k, gen):
         assert np.array_equal(i2, ei[s:s + n])
 
 
-@pytest.mark.parametrize("bucket", [1, 4, 32])
+@pytest.mark.parametrize("bucket", [1, 4, 32, 33, 96, 128])
 def test_knn_bucket_sizes(native, oracle, bucket):
     x, y, z = synth.scene(20000, 23)
     with _ctx(native, leaf_bucket=bucket) as c:
