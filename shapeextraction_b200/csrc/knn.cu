@@ -481,7 +481,9 @@ __device__ __forceinline__ void knn_warp(const float4* __restrict__ pts, const S
                 const uint32_t vote = __ballot_sync(FULL, act && dl <= dr);
                 const int nact = __popc(__ballot_sync(FULL, act));
                 const bool leftFirst = 2 * __popc(vote) >= nact;
-#pragma unroll
+                // rolled: one copy of the scan and merge code serves both
+                // children (a copy per child cost 4-8% in instruction fetch)
+#pragma unroll 1
                 for (int o = 0; o < 2; ++o) {
                     const bool left = (o == 0) == leftFirst;
                     const int32_t cnt = left ? cntl : cntr;
