@@ -33,17 +33,20 @@ namespace shapex {
 
 namespace {
 
-constexpr int kKnnThreads = 128;
-constexpr int kKnnWarps = kKnnThreads / 32;
 constexpr int kStackDepth = 96;
 // Per-k tile shape, measured on B200 (2M scene and 5M mixture clouds): small
 // lists leave registers for more resident warps, which pays for itself up to
-// k = 16; the 32-key list needs its registers (about 150), so it keeps the
-// larger buffer and 3 blocks per SM.
+// k = 16. The 24- and 32-key lists need their registers (about 144), so they
+// keep the larger buffer and run in 2-warp blocks: 7 resident blocks (14
+// warps) where 4-warp blocks fit only 3 (12 warps); k = 32 ran 2.7% faster.
+// min_blocks stays at 6 so that ptxas does not cap the registers (a cap of
+// 7 x 64 threads forced 128 registers and spills).
 template <int K>
 struct KnnCfg {
     static constexpr int buf = K <= 8 ? 40 : (K <= 16 ? 48 : 64);  // candidate buffer slots per lane
-    static constexpr int min_blocks = K <= 8 ? 6 : (K <= 16 ? 5 : 3);  // resident 128-thread blocks per SM
+    static constexpr int threads = K <= 16 ? 128 : 64;              // block size
+    static constexpr int warps = threads / 32;
+    static constexpr int min_blocks = K <= 8 ? 6 : (K <= 16 ? 5 : 6);  // resident blocks per SM asked of ptxas
 };
 constexpr int kMaxHalo = 48;            // seed points on each side of a warp's queries
 constexpr int kWindowMax = 32 + 2 * kMaxHalo;
@@ -572,14 +575,14 @@ __device__ __forceinline__ void knn_warp(const float4* __restrict__ pts, const S
 }
 
 template <int K, bool EXACT, bool EXT, bool NORMALS>
-__global__ void __launch_bounds__(kKnnThreads, KnnCfg<K>::min_blocks)
+__global__ void __launch_bounds__(KnnCfg<K>::threads, KnnCfg<K>::min_blocks)
     k_knn(const float4* __restrict__ pts, const SNode* __restrict__ snodes,
                                                      const uint64_t* __restrict__ codes, QArgs a, DevState* st) {
     extern __shared__ __align__(16) unsigned char knn_smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     using WS = WarpSmem<KnnCfg<K>::buf>;
     WS& W = reinterpret_cast<WS*>(knn_smem)[warp];
-    const int64_t q0 = ((int64_t)blockIdx.x * kKnnWarps + warp) * 32;
+    const int64_t q0 = ((int64_t)blockIdx.x * KnnCfg<K>::warps + warp) * 32;
     knn_warp<K, EXACT, EXT, NORMALS>(pts, snodes, codes, a, st, q0, W, lane);
 }
 
@@ -589,7 +592,7 @@ __global__ void __launch_bounds__(kKnnThreads, KnnCfg<K>::min_blocks)
 // start first and the small ones fill the tail. Each cloud's size is read on
 // the device from its own build state.
 template <int K, bool EXACT>
-__global__ void __launch_bounds__(kKnnThreads, KnnCfg<K>::min_blocks)
+__global__ void __launch_bounds__(KnnCfg<K>::threads, KnnCfg<K>::min_blocks)
     k_knn_batch(const BatchCloud* __restrict__ clouds, int n_clouds,
                                                            int64_t n_items, unsigned long long* counter, QArgs a) {
     extern __shared__ __align__(16) unsigned char knn_smem[];
@@ -619,18 +622,18 @@ __global__ void __launch_bounds__(kKnnThreads, KnnCfg<K>::min_blocks)
 
 template <int K, bool EXACT, bool EXT, bool NORMALS>
 cudaError_t launch_one(const BuildBufs& b, const QArgs& a, unsigned blocks, cudaStream_t s) {
-    constexpr int smem = (int)sizeof(WarpSmem<KnnCfg<K>::buf>) * kKnnWarps;
+    constexpr int smem = (int)sizeof(WarpSmem<KnnCfg<K>::buf>) * KnnCfg<K>::warps;
     cudaError_t e =
         cudaFuncSetAttribute(k_knn<K, EXACT, EXT, NORMALS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    k_knn<K, EXACT, EXT, NORMALS><<<blocks, kKnnThreads, smem, s>>>(b.pts4, b.snodes, b.codes, a, b.st);
+    k_knn<K, EXACT, EXT, NORMALS><<<blocks, KnnCfg<K>::threads, smem, s>>>(b.pts4, b.snodes, b.codes, a, b.st);
     return cudaGetLastError();
 }
 
 template <int K, bool EXACT>
 cudaError_t launch_k(const BuildBufs& b, const QArgs& a, bool ext, bool normals, cudaStream_t s) {
     const int64_t warps = (a.count + 31) / 32;
-    const unsigned blocks = (unsigned)((warps + kKnnWarps - 1) / kKnnWarps);
+    const unsigned blocks = (unsigned)((warps + KnnCfg<K>::warps - 1) / KnnCfg<K>::warps);
     if (ext) return launch_one<K, EXACT, true, false>(b, a, blocks, s);
     if (normals) return launch_one<K, EXACT, false, true>(b, a, blocks, s);
     return launch_one<K, EXACT, false, false>(b, a, blocks, s);
@@ -639,18 +642,18 @@ cudaError_t launch_k(const BuildBufs& b, const QArgs& a, bool ext, bool normals,
 template <int K, bool EXACT>
 cudaError_t launch_batch(const BatchCloud* clouds, int n_clouds, int64_t n_items, unsigned long long* counter,
                          const QArgs& a, cudaStream_t s, int num_sms) {
-    constexpr int smem = (int)sizeof(WarpSmem<KnnCfg<K>::buf>) * kKnnWarps;
+    constexpr int smem = (int)sizeof(WarpSmem<KnnCfg<K>::buf>) * KnnCfg<K>::warps;
     cudaError_t e = cudaFuncSetAttribute(k_knn_batch<K, EXACT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_knn_batch<K, EXACT>, kKnnThreads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_knn_batch<K, EXACT>, KnnCfg<K>::threads, smem);
     if (e != cudaSuccess) return e;
-    const int64_t want = (n_items + kKnnWarps - 1) / kKnnWarps;
+    const int64_t want = (n_items + KnnCfg<K>::warps - 1) / KnnCfg<K>::warps;
     const int64_t resident = (int64_t)(per_sm > 0 ? per_sm : 1) * num_sms;
     const unsigned blocks = (unsigned)(want < resident ? want : resident);
     e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s);
     if (e != cudaSuccess) return e;
-    k_knn_batch<K, EXACT><<<blocks, kKnnThreads, smem, s>>>(clouds, n_clouds, n_items, counter, a);
+    k_knn_batch<K, EXACT><<<blocks, KnnCfg<K>::threads, smem, s>>>(clouds, n_clouds, n_items, counter, a);
     return cudaGetLastError();
 }
 
