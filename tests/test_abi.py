@@ -65,6 +65,30 @@ def test_create_without_gpu_fails_cleanly(native):
         native.Context()
 
 
+def test_create_validates_options_before_the_device(native):
+    """se_create rejects bad options with SE_ERR_INVALID_ARG before it touches
+    a device, so the ranges are checked here too (leaf_bucket 1..128, seed
+    halo up to 48)."""
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    L = native.lib()
+
+    def create(**kw):
+        o = native.SeOptions()
+        L.se_options_init(ctypes.byref(o))
+        for k, v in kw.items():
+            setattr(o, k, v)
+        h = ctypes.c_void_p()
+        return L.se_create(ctypes.byref(h), ctypes.byref(o))
+
+    for bad in ({"leaf_bucket": 129}, {"leaf_bucket": -1}, {"seed_halo": 49}, {"code_bits": 32}):
+        assert create(**bad) == 1, bad
+    for ok in ({"leaf_bucket": 128}, {"leaf_bucket": 1}, {"leaf_bucket": 0}, {"seed_halo": 48}):
+        assert create(**ok) == 2, ok  # valid options: fails only at the missing device (SE_ERR_CUDA)
+
+
 def test_library_exports_only_the_c_abi(native):
     """Internal C++ helpers stay hidden; the exported se_ symbols are exactly
     the declared entry points."""
