@@ -302,74 +302,96 @@ __global__ void __launch_bounds__(kDedupThreads) k_dedup(const uint64_t* buf0, c
                                                          int code_bits, uint64_t* __restrict__ codes_out,
                                                          float4* __restrict__ pts4, float* __restrict__ pts3,
                                                          uint32_t* __restrict__ lookback, DevState* st) {
-    __shared__ uint32_t s_w[kDedupThreads / 32 + 1];
+    constexpr int kWarps = kDedupThreads / 32;
+    constexpr unsigned kFull = 0xffffffffu;
+    __shared__ uint32_t s_wcnt[kWarps];
     __shared__ uint32_t s_tile, s_excl;
     const uint64_t* __restrict__ keys = (st->n_active & 1) ? buf1 : buf0;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) s_tile = atomicAdd(&st->tile_counter[kSortPasses], 1u);
     __syncthreads();
     const uint32_t tile = s_tile;
-    const int64_t first = (int64_t)tile * kDedupTile + (int64_t)tid * kDedupIpt;
+    // Warp-striped: a warp's 32 * kDedupIpt keys are contiguous and element i
+    // of lane l is key wbase + 32 i + l, so loads and the compacted stores of
+    // each step are coalesced. Flags are kept as one ballot per step.
+    const int64_t wbase = (int64_t)tile * kDedupTile + (int64_t)warp * 32 * kDedupIpt;
     uint64_t k[kDedupIpt];
-    uint32_t flags = 0, c = 0;
-    uint64_t prev = first > 0 && first - 1 < n ? keys[first - 1] : ~0ull;
+    uint32_t m[kDedupIpt];
+    uint64_t last = (wbase > 0 && wbase - 1 < n) ? keys[wbase - 1] : 0ull;  // the key before this step's
+    uint32_t wcnt = 0;
 #pragma unroll
     for (int i = 0; i < kDedupIpt; ++i) {
-        const int64_t j = first + i;
+        const int64_t j = wbase + 32 * i + lane;
         k[i] = j < n ? keys[j] : 0ull;
-        const bool f = j < n && (j == 0 || k[i] != prev);
-        flags |= (uint32_t)f << i;
-        c += f;
-        prev = k[i];
+        uint64_t prev = __shfl_up_sync(kFull, k[i], 1);
+        if (lane == 0) prev = last;
+        last = __shfl_sync(kFull, k[i], 31);
+        m[i] = __ballot_sync(kFull, j < n && (j == 0 || k[i] != prev));
+        wcnt += __popc(m[i]);
     }
-    uint32_t tot;
-    const uint32_t toff = block_excl_scan<kDedupThreads, uint32_t>(c, s_w, &tot);
-    if (tid == 0) {
-        uint32_t* mine = lookback + tile;
+    if (lane == 0) s_wcnt[warp] = wcnt;
+    __syncthreads();
+    uint32_t woff = 0, tot = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+        const uint32_t c = s_wcnt[w];
+        woff += w < warp ? c : 0u;
+        tot += c;
+    }
+    // Decoupled look-back by warp 0, 32 predecessors per step: lane i reads
+    // tile p - i. The walk ends at the nearest tile with an inclusive prefix
+    // (tile 0 always publishes one); it needs every tile up to that one ready.
+    if (warp == 0) {
         uint32_t excl = 0;
         if (tile == 0) {
-            st_relaxed(mine, LB_PRE | tot);
+            if (lane == 0) st_relaxed(lookback, LB_PRE | tot);
         } else {
-            st_relaxed(mine, LB_AGG | tot);
+            if (lane == 0) st_relaxed(lookback + tile, LB_AGG | tot);
             int64_t p = (int64_t)tile - 1;
             int spins = 0;
-            while (p >= 0) {
-                const uint32_t v = ld_relaxed(lookback + p);
+            for (;;) {
+                const int64_t q = p - lane;
+                const uint32_t v = q >= 0 ? ld_relaxed(lookback + q) : LB_PRE;
                 const uint32_t f = v >> 30;
-                if (f == 0) {
-                    if (++spins > kSpinLimit) { set_err(&st->err, ERRBIT_LOOKBACK); break; }
+                const uint32_t pre = __ballot_sync(kFull, f == 2);
+                const uint32_t need = pre ? (((pre & (0u - pre)) << 1) - 1u) : kFull;  // lanes up to the first prefix
+                if (__ballot_sync(kFull, f == 0) & need) {
+                    if (++spins > kSpinLimit) {
+                        if (lane == 0) set_err(&st->err, ERRBIT_LOOKBACK);
+                        break;
+                    }
                     continue;
                 }
-                excl += v & LB_VAL;
-                if (f == 2) break;
-                --p;
+                excl += __reduce_add_sync(kFull, ((need >> lane) & 1u) ? (v & LB_VAL) : 0u);
+                if (pre) break;
+                p -= 32;
             }
-            st_relaxed(mine, LB_PRE | (excl + tot));
+            if (lane == 0) st_relaxed(lookback + tile, LB_PRE | (excl + tot));
         }
-        s_excl = excl;
-        const int64_t tile_end = (int64_t)(tile + 1) * kDedupTile;
-        if (tile_end >= n) st->u = (unsigned long long)(excl + tot);
+        if (lane == 0) {
+            s_excl = excl;
+            if ((int64_t)(tile + 1) * kDedupTile >= n) st->u = (unsigned long long)(excl + tot);
+        }
     }
     __syncthreads();
-    float mn, range;
-    mn = st->min_coord;
-    range = st->range;
-    uint32_t pos = s_excl + toff;
+    const float mn = st->min_coord, range = st->range;
+    uint32_t base = s_excl + woff;
 #pragma unroll
     for (int i = 0; i < kDedupIpt; ++i) {
-        if (flags & (1u << i)) {
+        if ((m[i] >> lane) & 1u) {
+            const uint32_t pos = base + __popc(m[i] & lanemask_lt());
             if ((int64_t)pos >= n) {
                 set_err(&st->err, ERRBIT_BOUNDS);
-                break;
+            } else {
+                codes_out[pos] = k[i];
+                const float3 p = code_to_point(k[i], mn, range, code_bits);
+                pts4[pos] = make_float4(p.x, p.y, p.z, 0.0f);
+                pts3[3 * (size_t)pos + 0] = p.x;
+                pts3[3 * (size_t)pos + 1] = p.y;
+                pts3[3 * (size_t)pos + 2] = p.z;
             }
-            codes_out[pos] = k[i];
-            const float3 p = code_to_point(k[i], mn, range, code_bits);
-            pts4[pos] = make_float4(p.x, p.y, p.z, 0.0f);
-            pts3[3 * (size_t)pos + 0] = p.x;
-            pts3[3 * (size_t)pos + 1] = p.y;
-            pts3[3 * (size_t)pos + 2] = p.z;
-            ++pos;
         }
+        base += __popc(m[i]);
     }
 }
 
