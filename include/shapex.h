@@ -81,8 +81,25 @@ typedef struct se_options {
                               graph and replays it while the batch layout, the k's and
                               the buffers repeat (inputs in device or pinned host
                               memory); 0: plain stream launches every call */
-    int32_t reserved[3];
+    /* Test hooks for the failure paths (all off by default; not for production
+     * use). The reference only prints its CUDA errors (src/CudaCommon.hpp:23-76);
+     * these make each bounded wait and each status path here reachable in a test
+     * without faulting or hanging a GPU. */
+    int32_t debug_wait_limit; /* 0: cross-block look-back waits give up after
+                                 2^22 polls; > 0: after this many */
+    int32_t debug_inject;     /* SE_DEBUG_* bits; each fires once, on the next call
+                                 that reaches it, and is then cleared */
+    int32_t reserved[1];
 } se_options;
+
+/* se_options.debug_inject bits. */
+#define SE_DEBUG_STALL_SORT_TILE 1 /* next se_build: the first radix-sort tile never
+                                      publishes its prefix, so its successors' waits run
+                                      out: SE_ERR_SYNC_TIMEOUT, nothing else is written */
+#define SE_DEBUG_SEARCH_LIMIT 2    /* next kNN call: each warp's tree walk gives up
+                                      after one node visit: SE_ERR_SEARCH_LIMIT */
+#define SE_DEBUG_ALLOC_FAIL 4      /* next growth of the build buffers fails as a failed
+                                      cudaMalloc would: SE_ERR_OOM */
 
 /* Sizes after se_build (RT::RadixTree / OT::Octree public fields). */
 typedef struct se_info {
@@ -261,12 +278,16 @@ SE_API int se_mlp_load(se_ctx* ctx, const char* path);
  * on every GPU that loads the library, held until the process exits).
  * - n may not exceed SE_STATIC_SORT_MAX_KEYS: larger n returns
  *   SE_ERR_INVALID_ARG and touches nothing.
- * - The first call on a device looks up the scratch's device address; make
- *   that first call before any stream capture on that device.
+ * - Every call looks up the scratch's device address in the current context
+ *   (cudaGetSymbolAddress), so it stays right after cudaDeviceReset or a
+ *   change of driver context.
  * - All calls on one device share the scratch: calls that overlap on the GPU
- *   (different streams or host threads, without ordering) race on it.
- * - Runs on `stream` (a cudaStream_t, NULL for the legacy default stream) and
- *   returns after the sort has finished. */
+ *   (different streams or host threads, without ordering) race on it. Each
+ *   call clears the parts of the scratch that must start at zero.
+ * - Synchronous: it runs on `stream` (a cudaStream_t, NULL for the legacy
+ *   default stream), reads the kernels' error word back and waits for the
+ *   stream before it returns. It must never be called while a stream is being
+ *   captured into a CUDA graph. */
 #define SE_STATIC_SORT_MAX_KEYS (1 << 20)
 #define SE_STATIC_SORT_BYTES (8u * (1u << 20) + 256u * 1024u + 20480u)
 SE_API int se_sort_keys_static(const uint64_t* d_keys_in, uint64_t* d_keys_out, int64_t n, void* stream);

@@ -10,11 +10,17 @@
 # (CCCL 2.8) in place of the empty cub submodule. Flags otherwise mirror a
 # release build of the reference (-O3 -DNDEBUG, --expt-relaxed-constexpr).
 #
-# Usage: oracle/build_ref.sh [reference_root]   (default /root/reference)
+# Usage: oracle/build_ref.sh [reference_root]
+#   The reference checkout is the argument, else $SHAPEX_REFERENCE_ROOT; there
+#   is no built-in default. Without either, a prebuilt refdriver is kept.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${1:-/root/reference}"
+REF="${1:-${SHAPEX_REFERENCE_ROOT:-}}"
 OUT="$HERE/_ref"
+if [ -z "$REF" ]; then
+    echo "no reference checkout given (argument or SHAPEX_REFERENCE_ROOT); keeping any prebuilt $OUT" >&2
+    exit 0
+fi
 SRC="$REF/src"
 if [ ! -d "$SRC" ]; then
     echo "reference sources not found at $SRC; keeping any prebuilt $OUT" >&2

@@ -292,34 +292,51 @@ struct KdTree {
     std::vector<KdNode> nodes;
     static constexpr int LEAF = 12;
 
-    int build(int b, int e) {
+    // Nodes of the subtree over m points (median splits: floor(m/2) left).
+    static int64_t count(int64_t m) { return m <= LEAF ? 1 : 1 + count(m / 2) + count(m - m / 2); }
+
+    // Subtree over perm[b, e) at node `id`, in depth-first preorder (left
+    // subtree at id + 1, right after it), so the layout is fixed by the sizes
+    // alone and large subtrees can be built as parallel tasks.
+    void build(int64_t b, int64_t e, int64_t id) {
         KdNode nd;
         for (int a = 0; a < 3; ++a) { nd.lo[a] = INFINITY; nd.hi[a] = -INFINITY; }
-        for (int i = b; i < e; ++i)
+        for (int64_t i = b; i < e; ++i)
             for (int a = 0; a < 3; ++a) {
                 nd.lo[a] = std::min(nd.lo[a], pts[3 * perm[i] + a]);
                 nd.hi[a] = std::max(nd.hi[a], pts[3 * perm[i] + a]);
             }
-        nd.begin = b; nd.end = e; nd.left = nd.right = -1;
-        int id = (int)nodes.size();
-        nodes.push_back(nd);
+        nd.begin = (int32_t)b; nd.end = (int32_t)e; nd.left = nd.right = -1;
         if (e - b > LEAF) {
             int ax = 0;
             float w = nd.hi[0] - nd.lo[0];
             for (int a = 1; a < 3; ++a) if (nd.hi[a] - nd.lo[a] > w) { w = nd.hi[a] - nd.lo[a]; ax = a; }
-            int mid = (b + e) / 2;
+            const int64_t mid = b + (e - b) / 2;
             std::nth_element(perm.begin() + b, perm.begin() + mid, perm.begin() + e,
                              [&](int32_t i, int32_t j) { return pts[3 * i + ax] < pts[3 * j + ax]; });
-            int l = build(b, mid);
-            int r = build(mid, e);
-            nodes[id].left = l; nodes[id].right = r;
+            nd.left = (int32_t)(id + 1);
+            nd.right = (int32_t)(id + 1 + count(mid - b));
+            if (e - b > 200000) {
+#pragma omp task
+                build(b, mid, nd.left);
+#pragma omp task
+                build(mid, e, nd.right);
+#pragma omp taskwait
+            } else {
+                build(b, mid, nd.left);
+                build(mid, e, nd.right);
+            }
         }
-        return id;
+        nodes[id] = nd;
     }
     KdTree(const float* p, int64_t n) : pts(p), perm(n) {
         std::iota(perm.begin(), perm.end(), 0);
-        nodes.reserve(2 * (n / LEAF + 1) + 8);
-        if (n > 0) build(0, (int)n);
+        if (n > 0) {
+            nodes.resize(count(n));
+#pragma omp parallel
+#pragma omp single
+            build(0, n, 0);
+        }
     }
 };
 

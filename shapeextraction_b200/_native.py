@@ -23,6 +23,10 @@ STATUS_NAMES = {
 }
 SE_MEM_HOST = 0
 SE_MEM_DEVICE = 1
+# se_options.debug_inject bits (test hooks for the failure paths)
+SE_DEBUG_STALL_SORT_TILE = 1
+SE_DEBUG_SEARCH_LIMIT = 2
+SE_DEBUG_ALLOC_FAIL = 4
 
 # Every entry point declared in include/shapex.h.
 EXPORTS = [
@@ -47,7 +51,8 @@ class SeOptions(ctypes.Structure):
         ("viewpoint", ctypes.c_float * 3), ("eigengap_fp64", ctypes.c_float), ("leaf_bucket", ctypes.c_int32),
         ("device", ctypes.c_int32), ("stream", ctypes.c_void_p), ("seed_halo", ctypes.c_int32),
         ("learned", ctypes.c_int32), ("learned_skip_seed", ctypes.c_int32), ("search_compat", ctypes.c_int32),
-        ("batch_graph", ctypes.c_int32), ("reserved", ctypes.c_int32 * 3),
+        ("batch_graph", ctypes.c_int32), ("debug_wait_limit", ctypes.c_int32),
+        ("debug_inject", ctypes.c_int32), ("reserved", ctypes.c_int32 * 1),
     ]
 
 
@@ -162,7 +167,8 @@ class Context:
 
     def __init__(self, code_bits=63, root_compat=True, build_octree=True, viewpoint=(0.0, 0.0, 0.0),
                  eigengap_fp64=1e-4, leaf_bucket=96, device=0, stream=None, seed_halo=-1, learned=False,
-                 learned_skip_seed=False, search_compat=False, batch_graph=True):
+                 learned_skip_seed=False, search_compat=False, batch_graph=True, debug_wait_limit=0,
+                 debug_inject=0):
         L = lib()
         o = SeOptions()
         L.se_options_init(ctypes.byref(o))
@@ -180,6 +186,8 @@ class Context:
         o.learned_skip_seed = int(bool(learned_skip_seed))
         o.search_compat = int(bool(search_compat))
         o.batch_graph = int(bool(batch_graph))
+        o.debug_wait_limit = int(debug_wait_limit)
+        o.debug_inject = int(debug_inject)
         self.options = o
         h = ctypes.c_void_p()
         rc = L.se_create(ctypes.byref(h), ctypes.byref(o))

@@ -192,8 +192,10 @@ struct SortSmem {
 };
 
 __global__ void __launch_bounds__(kSortThreads) k_onesweep(uint64_t* buf0, uint64_t* buf1, int64_t n, int pass,
-                                                           uint32_t* __restrict__ lookback, DevState* st) {
-    if (!st->pass_active[pass]) return;
+                                                           uint32_t* __restrict__ lookback, DevState* st,
+                                                           int spin_limit, int stall_first_tile) {
+    // a look-back of this build gave up: its key order is lost, write nothing
+    if (!st->pass_active[pass] || (st->err & ERRBIT_LOOKBACK)) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SortSmem& S = *reinterpret_cast<SortSmem*>(smem_raw);
     const int parity = st->pass_parity[pass];
@@ -245,7 +247,7 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(uint64_t* buf0, uint6
     if (tid < 256) {
         uint32_t* mine = lookback + (size_t)tile * 256 + tid;
         if (tile == 0) {
-            st_relaxed(mine, LB_PRE | cnt);
+            if (!stall_first_tile) st_relaxed(mine, LB_PRE | cnt);
         } else {
             st_relaxed(mine, LB_AGG | cnt);
             int64_t p = (int64_t)tile - 1;
@@ -254,7 +256,7 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(uint64_t* buf0, uint6
                 const uint32_t v = ld_relaxed(lookback + (size_t)p * 256 + tid);
                 const uint32_t f = v >> 30;
                 if (f == 0) {
-                    if (++spins > kSpinLimit) { set_err(&st->err, ERRBIT_LOOKBACK); break; }
+                    if (++spins > spin_limit) { set_err(&st->err, ERRBIT_LOOKBACK); break; }
                     continue;
                 }
                 excl += v & LB_VAL;
@@ -301,7 +303,10 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(uint64_t* buf0, uint6
 __global__ void __launch_bounds__(kDedupThreads) k_dedup(const uint64_t* buf0, const uint64_t* buf1, int64_t n,
                                                          int code_bits, uint64_t* __restrict__ codes_out,
                                                          float4* __restrict__ pts4, float* __restrict__ pts3,
-                                                         uint32_t* __restrict__ lookback, DevState* st) {
+                                                         uint32_t* __restrict__ lookback, DevState* st,
+                                                         int spin_limit) {
+    // a sort look-back gave up: no order to dedup; u stays 0 and later stages do nothing
+    if (st->err & ERRBIT_LOOKBACK) return;
     constexpr int kWarps = kDedupThreads / 32;
     constexpr unsigned kFull = 0xffffffffu;
     __shared__ uint32_t s_wcnt[kWarps];
@@ -356,7 +361,7 @@ __global__ void __launch_bounds__(kDedupThreads) k_dedup(const uint64_t* buf0, c
                 const uint32_t pre = __ballot_sync(kFull, f == 2);
                 const uint32_t need = pre ? (((pre & (0u - pre)) << 1) - 1u) : kFull;  // lanes up to the first prefix
                 if (__ballot_sync(kFull, f == 0) & need) {
-                    if (++spins > kSpinLimit) {
+                    if (++spins > spin_limit) {
                         if (lane == 0) set_err(&st->err, ERRBIT_LOOKBACK);
                         break;
                     }
@@ -623,7 +628,7 @@ __global__ void __launch_bounds__(kScanThreads) k_oct_scan(const uint8_t* __rest
                                                            int32_t* __restrict__ counts,
                                                            int32_t* __restrict__ offsets,
                                                            unsigned long long* __restrict__ lookback,
-                                                           DevState* st) {
+                                                           DevState* st, int spin_limit) {
     __shared__ long long s_w[kScanThreads / 32 + 1];
     __shared__ uint32_t s_tile;
     __shared__ long long s_excl;
@@ -668,7 +673,7 @@ __global__ void __launch_bounds__(kScanThreads) k_oct_scan(const uint8_t* __rest
                 const unsigned long long v = ld_relaxed64(lookback + p);
                 const unsigned long long f = v >> 62;
                 if (f == 0) {
-                    if (++spins > kSpinLimit) { set_err(&st->err, ERRBIT_LOOKBACK); break; }
+                    if (++spins > spin_limit) { set_err(&st->err, ERRBIT_LOOKBACK); break; }
                     continue;
                 }
                 excl += sx62(v & LB64_VAL);
@@ -869,7 +874,8 @@ cudaError_t enqueue_sort_keys(uint64_t* keys, uint64_t* tmp, int64_t n, uint32_t
     const int64_t sort_tiles = (n + kSortTile - 1) / kSortTile;
     for (int pass = 0; pass < kSortPasses; ++pass) {
         cudaMemsetAsync(lookback, 0, sizeof(uint32_t) * 256 * sort_tiles, s);
-        k_onesweep<<<(unsigned)sort_tiles, kSortThreads, sizeof(SortSmem), s>>>(keys, tmp, n, pass, lookback, st);
+        k_onesweep<<<(unsigned)sort_tiles, kSortThreads, sizeof(SortSmem), s>>>(keys, tmp, n, pass, lookback, st,
+                                                                                 kSpinLimit, 0);
     }
     k_copy_if_odd<<<grid_for(n, 256, num_sms * 4), 256, 0, s>>>(tmp, keys, n, st);
     return cudaGetLastError();
@@ -881,7 +887,7 @@ cudaError_t enqueue_octree(const BuildBufs& b, const BuildParams& p, cudaStream_
     cudaMemsetAsync(b.lookback64, 0, sizeof(unsigned long long) * scan_tiles, s);
     cudaMemsetAsync(&b.st->tile_counter[kSortPasses + 1], 0, sizeof(uint32_t), s);
     k_oct_scan<<<(unsigned)scan_tiles, kScanThreads, 0, s>>>(b.prefix_n, b.parent, b.oct_counts, b.oct_offsets,
-                                                             b.lookback64, b.st);
+                                                             b.lookback64, b.st, p.spin_limit);
     k_oct_zero<<<grid_for(b.oct_cap * 7, 256, num_sms * 8), 256, 0, s>>>((OtNode*)b.oct_nodes, b.oct_cap, b.st);
     k_oct_make<<<grid_for(n, 256, 0), 256, 0, s>>>((OtNode*)b.oct_nodes, b.oct_cap, b.oct_offsets, b.oct_counts,
                                                    b.codes, b.prefix_n, b.parent, p.code_bits, b.st);
@@ -895,8 +901,14 @@ cudaError_t enqueue_octree(const BuildBufs& b, const BuildParams& p, cudaStream_
 cudaError_t enqueue_build(const BuildBufs& b, const BuildParams& p, cudaStream_t s, int num_sms, cudaEvent_t* ev,
                           int* launches) {
     int nl = 0;
+    // stage i runs between events i and i+1; each stage is also an NVTX range
+    static const char* const kStageNames[kBuildEvents - 1] = {
+        "shapex.build.bbox", "shapex.build.encode", "shapex.build.sort", "shapex.build.dedup",
+        "shapex.build.radix_tree", "shapex.build.search_boxes", "shapex.build.octree"};
     auto mark = [&](int i) {
         if (ev) cudaEventRecord(ev[i], s);
+        if (i > 0) nvtxRangePop();
+        if (i < kBuildEvents - 1) nvtxRangePushA(kStageNames[i]);
     };
     {
         // per device and cheap: set on every build
@@ -922,14 +934,15 @@ cudaError_t enqueue_build(const BuildBufs& b, const BuildParams& p, cudaStream_t
     for (int pass = 0; pass < kSortPasses; ++pass) {
         cudaMemsetAsync(b.lookback, 0, sizeof(uint32_t) * 256 * sort_tiles, s);
         k_onesweep<<<(unsigned)sort_tiles, kSortThreads, sizeof(SortSmem), s>>>(b.keys0, b.keys1, n, pass,
-                                                                                 b.lookback, b.st);
+                                                                                 b.lookback, b.st, p.spin_limit,
+                                                                                 p.stall_first_tile);
         ++nl;
     }
     mark(3);
     const int64_t dd_tiles = (n + kDedupTile - 1) / kDedupTile;
     cudaMemsetAsync(b.lookback, 0, sizeof(uint32_t) * dd_tiles, s);
     k_dedup<<<(unsigned)dd_tiles, kDedupThreads, 0, s>>>(b.keys0, b.keys1, n, p.code_bits, b.codes, b.pts4, b.pts3,
-                                                         b.lookback, b.st);
+                                                         b.lookback, b.st, p.spin_limit);
     ++nl;
     mark(4);
     cudaMemsetAsync(b.parent, 0, sizeof(int32_t) * n, s);
@@ -952,7 +965,10 @@ cudaError_t enqueue_build(const BuildBufs& b, const BuildParams& p, cudaStream_t
     mark(6);
     if (p.build_octree) {
         cudaError_t e = enqueue_octree(b, p, s, num_sms, &nl);
-        if (e != cudaSuccess) return e;
+        if (e != cudaSuccess) {
+            nvtxRangePop();  // the octree stage's range
+            return e;
+        }
     }
     mark(7);
     if (launches) *launches = nl;

@@ -83,6 +83,10 @@ void free_build(se_ctx* c) {
 int ensure_build_capacity(se_ctx* c, int64_t n) {
     if (n <= c->cap && c->b.keys0) return SE_OK;
     free_build(c);
+    if (c->debug_pending & SE_DEBUG_ALLOC_FAIL) {  // test hook: this growth fails as cudaMalloc would
+        c->debug_pending &= ~SE_DEBUG_ALLOC_FAIL;
+        return cuda_fail(c, cudaErrorMemoryAllocation, "alloc keys (injected by SE_DEBUG_ALLOC_FAIL)");
+    }
     const int64_t cap = n < 1024 ? 1024 : n;
     BuildBufs& b = c->b;
     const int64_t sort_tiles = (cap + kSortTile - 1) / kSortTile;
@@ -161,6 +165,10 @@ int run_query(se_ctx* c, int k, int64_t start, int64_t count, const float* ext, 
     q.seed_halo = seed_halo_for(c, k);
     q.compat = c->opt.search_compat ? 1 : 0;
     q.n_octree = c->info.n_octree;
+    if (c->debug_pending & SE_DEBUG_SEARCH_LIMIT) {  // test hook: one node visit per warp
+        c->debug_pending &= ~SE_DEBUG_SEARCH_LIMIT;
+        q.step_limit = 1;
+    }
     if (q.compat && q.n_octree < 1)
         return fail(c, SE_ERR_UNSUPPORTED, "the reference-compatible search needs the octree (build_octree = 1, u >= 2)");
     const bool use_learned = c->opt.learned && !ext && c->mlp_ready && !q.compat;
@@ -311,8 +319,12 @@ int se_create(se_ctx** out, const se_options* opt) {
     if (o.seed_halo < 0) o.seed_halo = -1;  // per-k default, resolved by seed_halo_for
     if (o.seed_halo > 48) return SE_ERR_INVALID_ARG;
     if (!(o.eigengap_fp64 >= 0.0f)) return SE_ERR_INVALID_ARG;
+    if (o.debug_wait_limit < 0) return SE_ERR_INVALID_ARG;
+    if (o.debug_inject & ~(SE_DEBUG_STALL_SORT_TILE | SE_DEBUG_SEARCH_LIMIT | SE_DEBUG_ALLOC_FAIL))
+        return SE_ERR_INVALID_ARG;
     se_ctx* c = new se_ctx();
     c->opt = o;
+    c->debug_pending = o.debug_inject;
     cudaError_t e = cudaSetDevice(o.device);
     int major = 0;
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, o.device);
@@ -403,6 +415,7 @@ int se_destroy(se_ctx* c) {
 const char* se_last_error(const se_ctx* c) { return c ? c->last_error.c_str() : "null context"; }
 
 int se_build(se_ctx* c, const float* x, const float* y, const float* z, int64_t n, int mem) {
+    NvtxRange nvtx("shapex.se_build");
     if (int rc = prologue(c)) return rc;
     c->built = false;
     if (int rc = check_mem(c, mem)) return rc;
@@ -426,10 +439,17 @@ int se_build(se_ctx* c, const float* x, const float* y, const float* z, int64_t 
         b.z = z;
     }
     BuildParams p{n, c->opt.code_bits, c->opt.root_compat, c->opt.build_octree, c->opt.leaf_bucket};
+    if (c->opt.debug_wait_limit > 0) p.spin_limit = c->opt.debug_wait_limit;
+    if (c->debug_pending & SE_DEBUG_STALL_SORT_TILE) {  // test hook: the first sort tile never publishes
+        c->debug_pending &= ~SE_DEBUG_STALL_SORT_TILE;
+        p.stall_first_tile = 1;
+    }
     c->have_build_times = false;
     SE_CUDA(c, enqueue_build(b, p, c->stream, c->num_sms, c->build_ev, &c->build_launches), "launch build");
     if (int rc = read_state(c)) return rc;
     c->have_build_times = true;
+    // any other failure first: the octree count of a failed build means nothing
+    if (int rc = check_err_bits(c, c->h_st->err & ~(uint32_t)ERRBIT_OCT_CAPACITY)) return rc;
     if (c->h_st->err & ERRBIT_OCT_CAPACITY) {
         const int64_t m = (int64_t)c->h_st->n_oct;
         if (int rc = ensure_oct_capacity(c, m)) return rc;
@@ -528,12 +548,14 @@ int se_get_points(se_ctx* c, float* out, int mem) {
 }
 
 int se_knn_self(se_ctx* c, int k, int64_t start, int64_t count, int32_t* out_idx, float* out_d2, int mem) {
+    NvtxRange nvtx("shapex.se_knn_self");
     if (int rc = prologue(c)) return rc;
     if (!out_idx && count > 0) return fail(c, SE_ERR_INVALID_ARG, "null output");
     return run_query(c, k, start, count, nullptr, out_idx, out_d2, nullptr, mem);
 }
 
 int se_knn(se_ctx* c, int k, const float* queries, int64_t nq, int32_t* out_idx, float* out_d2, int mem) {
+    NvtxRange nvtx("shapex.se_knn");
     if (int rc = prologue(c)) return rc;
     if (nq > 0 && (!queries || !out_idx)) return fail(c, SE_ERR_INVALID_ARG, "null pointer");
     if (nq == 0) return SE_OK;
@@ -541,6 +563,7 @@ int se_knn(se_ctx* c, int k, const float* queries, int64_t nq, int32_t* out_idx,
 }
 
 int se_normals(se_ctx* c, int k, int64_t start, int64_t count, float* out, int mem) {
+    NvtxRange nvtx("shapex.se_normals");
     if (int rc = prologue(c)) return rc;
     if (!out && count > 0) return fail(c, SE_ERR_INVALID_ARG, "null output");
     return run_query(c, k, start, count, nullptr, nullptr, nullptr, out, mem);

@@ -189,6 +189,7 @@ int enqueue_batch(se_ctx* c, const BatchPlan& plan, const BatchCloud* d_desc, co
 
 int se_normals_batch(se_ctx* c, const float* x, const float* y, const float* z, const int64_t* offsets, int n_clouds,
                      const int32_t* ks, float* out_normals, int64_t* out_u, int mem) {
+    NvtxRange nvtx("shapex.se_normals_batch");
     if (int rc = prologue(c)) return rc;
     if (int rc = check_mem(c, mem)) return rc;
     if (n_clouds < 0 || (n_clouds > 0 && (!offsets || !ks || !out_u)))

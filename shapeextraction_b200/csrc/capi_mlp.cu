@@ -212,6 +212,7 @@ int se_mlp_grad(se_ctx* c, const float* features, const float* targets, int64_t 
 
 int se_mlp_train(se_ctx* c, const float* features, const float* targets, int64_t n, int steps, int batch, float lr,
                  float* losses, int mem) {
+    NvtxRange nvtx("shapex.se_mlp_train");
     if (int rc = prologue(c)) return rc;
     if (int rc = check_mem(c, mem)) return rc;
     if (!c->mlp_ready) return fail(c, SE_ERR_NOT_BUILT, "model not initialised");

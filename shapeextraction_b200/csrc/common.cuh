@@ -4,8 +4,18 @@
 #include <cstdint>
 #include <cstring>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 namespace shapex {
+
+// NVTX range for the host side of one API call or build stage (header-only
+// NVTX 3: a no-op unless a profiler is attached).
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Error bits kernels OR into the context's device error word.
 enum : uint32_t {
@@ -17,7 +27,8 @@ enum : uint32_t {
     ERRBIT_OCT_CAPACITY = 1u << 5,  // octree larger than its buffer (host regrows)
 };
 
-// Iteration cap for every spin-wait on another block's flag.
+// Iteration cap for every spin-wait on another block's flag (the default;
+// a context's debug_wait_limit option can lower it for tests).
 constexpr int kSpinLimit = 1 << 22;
 
 __device__ __forceinline__ void set_err(uint32_t* err, uint32_t bit) { atomicOr(err, bit); }

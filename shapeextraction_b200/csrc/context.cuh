@@ -59,6 +59,7 @@ struct se_ctx {
     DevState* h_st = nullptr;   // pinned mirror of the device state
 
     bool built = false;
+    int debug_pending = 0;  // SE_DEBUG_* test hooks not fired yet (from options.debug_inject)
     se_info info{};
     int64_t last_counters[kQueryCounters] = {};
 

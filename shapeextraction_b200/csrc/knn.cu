@@ -158,6 +158,7 @@ struct QArgs {
     const float* learned_r2;
     int learned_skip_seed;
     int device_count;  // 1: u = count = the build's unique-point count, read on the device (start 0)
+    int step_limit;    // > 0: node visits per warp before the walk gives up (test hook)
 };
 
 struct Counters {
@@ -455,7 +456,8 @@ __device__ __forceinline__ void knn_warp(const float4* __restrict__ pts, const S
             int sp = 1;
             if (lane == 0) W.stack[0] = 0;
             __syncwarp();
-            const uint32_t step_cap = (uint32_t)min64(2 * u + 64, 0x7fffffff);
+            const uint32_t step_cap =
+                a.step_limit > 0 ? (uint32_t)a.step_limit : (uint32_t)min64(2 * u + 64, 0x7fffffff);
             while (sp > 0) {
                 --sp;
                 const int32_t node = W.stack[sp];
@@ -729,6 +731,7 @@ cudaError_t enqueue_query(const BuildBufs& b, const QueryParams& q, cudaStream_t
     a.learned_r2 = q.learned_r2;
     a.learned_skip_seed = q.learned_skip_seed;
     a.device_count = q.device_count;
+    a.step_limit = q.step_limit;
     if (a.seed_halo > kMaxHalo) a.seed_halo = kMaxHalo;
     if (a.seed_halo < 0) a.seed_halo = 0;
     const bool ext = q.ext_queries != nullptr;

@@ -107,6 +107,8 @@ struct BuildParams {
     int root_compat;
     int build_octree;
     int bucket;
+    int spin_limit = kSpinLimit;  // polls before a look-back wait gives up
+    int stall_first_tile = 0;     // test hook: the first sort tile never publishes its prefix
 };
 
 // Stage events of one build: [0] start, then after bbox, encode, sort, dedup,
@@ -181,6 +183,7 @@ struct QueryParams {
                               // is then an upper bound used only to size the grid
     int compat;               // 1: the reference's approximate octree search and FP32 covariance
     int64_t n_octree;         // octree nodes (compat search)
+    int step_limit = 0;       // > 0: node visits per warp before the walk gives up (test hook)
 };
 
 cudaError_t enqueue_query(const BuildBufs& b, const QueryParams& q, cudaStream_t s, int num_sms);

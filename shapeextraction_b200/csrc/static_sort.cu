@@ -15,7 +15,6 @@
 //   then              the sort's small device state (histograms, counters)
 
 #include <cstdint>
-#include <mutex>
 
 #include "pipeline.cuh"
 #include "shapex.h"
@@ -36,25 +35,19 @@ static_assert(kStateOffset + sizeof(DevState) <= kScratchBytes, "scratch layout 
 // device address: the address is looked up with cudaGetSymbolAddress below.
 static __device__ __align__(256) unsigned char g_sort_scratch[kScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mutex;
-void* g_scratch_addr[kMaxDevices] = {};
-
-// Device address of the scratch on the current device, looked up on the first
-// call made on that device (with that device current).
-int scratch_address(int device, void** out) {
-    if (device < 0 || device >= kMaxDevices) return SE_ERR_UNSUPPORTED;
-    std::lock_guard<std::mutex> lock(g_mutex);
-    if (!g_scratch_addr[device]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_sort_scratch);
-        if (e != cudaSuccess || p == nullptr) {
-            cudaGetLastError();
-            return SE_ERR_CUDA;
-        }
-        g_scratch_addr[device] = p;
+// Device address of the scratch in the current context. It is looked up on
+// every call, not cached: after cudaDeviceReset, or when the caller makes
+// another driver context current on the same device, the library's module is
+// loaded again and the array can move, so a cached address could point at
+// memory the array no longer owns.
+int scratch_address(void** out) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_sort_scratch);
+    if (e != cudaSuccess || p == nullptr) {
+        cudaGetLastError();
+        return SE_ERR_CUDA;
     }
-    *out = g_scratch_addr[device];
+    *out = p;
     return SE_OK;
 }
 
@@ -70,7 +63,7 @@ extern "C" int se_sort_keys_static(const uint64_t* d_keys_in, uint64_t* d_keys_o
         return SE_ERR_CUDA;
     }
     void* base = nullptr;
-    if (int rc = scratch_address(device, &base)) return rc;
+    if (int rc = scratch_address(&base)) return rc;
     unsigned char* b = static_cast<unsigned char*>(base);
     uint64_t* tmp = reinterpret_cast<uint64_t*>(b);
     uint32_t* lookback = reinterpret_cast<uint32_t*>(b + kKeyBytes);

@@ -45,18 +45,29 @@ def _device_for(group):
     return torch.device("cpu")
 
 
+def _global_rank(group, group_rank: int) -> int:
+    """The global rank of `group_rank` in `group` (collectives take global ranks)."""
+    import torch.distributed as dist
+
+    if group is None or group is dist.group.WORLD:
+        return group_rank
+    return dist.get_global_rank(group, group_rank)
+
+
 def broadcast_cloud(x, y, z, group=None, root: int = 0):
     """The root's coordinates on every rank, as float32 tensors on the
-    group's device (the other ranks may pass None)."""
+    group's device (the other ranks may pass None). `root` is a rank within
+    `group` (the default group: a global rank)."""
     import torch
     import torch.distributed as dist
 
     dev = _device_for(group)
     rank = dist.get_rank(group)
+    src = _global_rank(group, root)
     n = torch.zeros(1, dtype=torch.int64, device=dev)
     if rank == root:
         n[0] = len(x)
-    dist.broadcast(n, src=root, group=group)
+    dist.broadcast(n, src=src, group=group)
     n = int(n[0])
     out = []
     for v in (x, y, z):
@@ -65,7 +76,7 @@ def broadcast_cloud(x, y, z, group=None, root: int = 0):
             t = t.to(dev).contiguous()
         else:
             t = torch.empty(n, dtype=torch.float32, device=dev)
-        dist.broadcast(t, src=root, group=group)
+        dist.broadcast(t, src=src, group=group)
         out.append(t)
     return tuple(out)
 
@@ -74,7 +85,8 @@ def sharded_normals(ctx, x, y, z, k: int, group=None, root: int = 0):
     """Normals of all u unique points (Morton order) on every rank, each rank
     computing one contiguous range. `ctx` is this rank's Context (or any
     object with build / info / normals of the same meaning); x, y, z are the
-    root rank's coordinates (ignored elsewhere)."""
+    root rank's coordinates (ignored elsewhere); `root` is a rank within
+    `group`."""
     import torch
     import torch.distributed as dist
 

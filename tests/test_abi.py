@@ -83,9 +83,11 @@ def test_create_validates_options_before_the_device(native):
         h = ctypes.c_void_p()
         return L.se_create(ctypes.byref(h), ctypes.byref(o))
 
-    for bad in ({"leaf_bucket": 129}, {"leaf_bucket": -1}, {"seed_halo": 49}, {"code_bits": 32}):
+    for bad in ({"leaf_bucket": 129}, {"leaf_bucket": -1}, {"seed_halo": 49}, {"code_bits": 32},
+                {"debug_wait_limit": -1}, {"debug_inject": 8}):
         assert create(**bad) == 1, bad
-    for ok in ({"leaf_bucket": 128}, {"leaf_bucket": 1}, {"leaf_bucket": 0}, {"seed_halo": 48}):
+    for ok in ({"leaf_bucket": 128}, {"leaf_bucket": 1}, {"leaf_bucket": 0}, {"seed_halo": 48},
+               {"debug_wait_limit": 100}, {"debug_inject": 7}):
         assert create(**ok) == 2, ok  # valid options: fails only at the missing device (SE_ERR_CUDA)
 
 
@@ -102,3 +104,15 @@ def test_library_exports_only_the_c_abi(native):
     names = [ln.split()[-1] for ln in out.stdout.splitlines() if ln.strip()]
     assert sorted(n for n in names if n.startswith("se_")) == header_functions()
     assert not [n for n in names if "shapex" in n]
+
+
+def test_static_sort_source_allocates_nothing():
+    """se_sort_keys_static's translation unit calls no allocating routine: its
+    scratch is the file-scope static device array, addressed per call."""
+    src = open(os.path.join(ROOT, "shapeextraction_b200", "csrc", "static_sort.cu")).read()
+    code = re.sub(r"//[^\n]*", "", src)
+    for name in ("cudaMalloc", "cudaMallocAsync", "cudaMallocManaged", "cudaMallocHost", "cudaHostAlloc",
+                 "cudaFree", "malloc(", "new ", "regrow("):
+        assert name not in code, name
+    assert "static __device__ __align__(256)" in code
+    assert code.count("cudaGetSymbolAddress") == 1

@@ -119,3 +119,41 @@ def test_batch_large_and_small_clouds(native, graph):
             c.build(x, y, z)
             assert u[i] == c.info()["n_points"]
             assert np.array_equal(nrm[offsets[i]:offsets[i] + u[i]], c.normals(int(ks[i]))), i
+
+
+def test_batch_256_sampled_clouds_vs_oracle(native, oracle):
+    """The batched configuration itself (256 scenes, sizes log-uniform in
+    [1k, 500k], k per cloud from {8, 16, 32}; the bench's seed), checked
+    against the CPU oracle rather than against single-cloud calls: for 8
+    clouds of each k, spread over the sizes, the batch's u and normals (within
+    1e-3 rad of FP64 where the FP64 relative eigengap exceeds 1e-4, with the
+    reference's sign rule) and the cloud's self-query kNN lists (bit-exact)."""
+    from conftest import angle_deg_free
+
+    clouds, ks = synth.batched_clouds(256, 1)
+    ks = np.ascontiguousarray(ks, np.int32)
+    with native.Context() as c:
+        nrm, offsets, u = c.normals_batch(clouds, ks)
+        sizes = np.array([cl[0].size for cl in clouds])
+        for k in (8, 16, 32):
+            ids = np.flatnonzero(ks == k)
+            ids = ids[np.argsort(sizes[ids])]
+            pick = ids[np.linspace(0, ids.size - 1, min(8, ids.size)).astype(int)]
+            for i in pick:
+                x, y, z = clouds[i]
+                ref = oracle.build_stages(x, y, z)
+                pts = ref["points"]
+                assert u[i] == pts.shape[0], i
+                ei, ed = oracle.knn_exact(pts, pts, k)
+                got = nrm[offsets[i]:offsets[i] + u[i]]
+                nref, ev = oracle.normals_f64(pts, ei, pts)
+                gap = (ev[:, 1] - ev[:, 0]) / np.maximum(np.abs(ev[:, 2]), 1e-300)
+                good = gap > 1e-4
+                assert good.mean() > 0.5, i
+                assert angle_deg_free(got[good], nref[good]).max() <= 1e-3, i
+                d = np.sum(-pts.astype(np.float64) * nref, axis=1)
+                clear = good & (np.abs(d) > 1e-4)
+                assert np.all(np.sum(got[clear] * nref[clear], axis=1) > 0), i
+                c.build(x, y, z)
+                idx, d2 = c.knn_self(k, with_d2=True)
+                assert np.array_equal(d2, ed) and np.array_equal(idx, ei), i

@@ -75,6 +75,45 @@ def test_sharded_normals_two_gloo_ranks(n):
         assert np.array_equal(results[r], want)
 
 
+def _subgroup_worker(rank, world, port, n, results):
+    import torch.distributed as dist
+
+    from shapeextraction_b200.distributed import sharded_normals
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        # a subgroup of global ranks {1, 2}; its rank 0 (global rank 1) is the root
+        sub = dist.new_group([1, 2])
+        if rank in (1, 2):
+            rng = np.random.default_rng(0)
+            x, y, z = (rng.integers(0, 50, n).astype(np.float32) for _ in range(3)) if rank == 1 else (None,) * 3
+            out = sharded_normals(_StubContext(), x, y, z, 8, group=sub, root=0)
+            results[rank] = out.numpy()
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_normals_subgroup_root_is_a_group_rank():
+    """`root` names a rank of the group, not a global rank: in a subgroup of
+    global ranks {1, 2}, root 0 is global rank 1, the only rank holding data."""
+    import torch.multiprocessing as mp
+
+    n = 777
+    mgr = mp.Manager()
+    results = mgr.dict()
+    mp.spawn(_subgroup_worker, args=(3, _free_port(), n, results), nprocs=3, join=True)
+    rng = np.random.default_rng(0)
+    x, y, z = (rng.integers(0, 50, n).astype(np.float32) for _ in range(3))
+    u = _StubContext().build(x, y, z)["n_points"]
+    want = _StubContext().normals(8, 0, u)
+    assert sorted(results.keys()) == [1, 2]
+    for r in (1, 2):
+        assert np.array_equal(results[r], want)
+
+
 @pytest.mark.gpu
 def test_sharded_normals_one_nccl_rank(native):
     import torch

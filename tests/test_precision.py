@@ -4,8 +4,10 @@ near-degenerate neighbourhoods (anisotropic-noise planes, collinear segments,
 with the FP64 oracle (exact kNN set, FP64 covariance and Jacobi) on a sample
 of queries; angular errors are reported separately by the oracle's relative
 eigengap (l1 - l0) / l2, for the FP64-redo threshold of the configuration
-(1e-6) and the library default (1e-4). Set SHAPEX_REPORT_DIR to keep the
-report as JSON."""
+(1e-6) and the library default (1e-4). At the configuration's threshold the
+self-query kNN path (the one that produces the normals) is checked bit-exact
+on 64 Morton-contiguous slices, plain and with the learned radius. Set
+SHAPEX_REPORT_DIR to keep the report as JSON."""
 import json
 import os
 
@@ -13,7 +15,8 @@ import numpy as np
 import pytest
 
 from conftest import angle_deg_free
-from shapeextraction_b200 import synth
+from shapeextraction_b200 import learned, synth
+from test_configs import check_knn_rows, slices
 
 pytestmark = pytest.mark.gpu
 
@@ -45,9 +48,25 @@ def test_precision_mix_20M(native, oracle):
                 c2.build(x, y, z)
                 nrm = c2.normals(16)
                 fp64 = c2.stats()["fp64_solves"]  # counters of the last query call
-                idx = c2.knn(pts[q], 16) if thr == 1e-4 else None
-            if idx is not None:
-                assert np.array_equal(idx, ei)  # exact kNN on the sample
+                if thr == 1e-4:
+                    # external queries at the sampled points find the same lists
+                    assert np.array_equal(c2.knn(pts[q], 16), ei)
+                else:
+                    # the configuration's own threshold, as the bench runs it:
+                    # the self-query path (the rows that produce the normals)
+                    # bit-exact on 64 Morton-contiguous slices, plain and with
+                    # the learned radius, whose normals equal the plain ones
+                    ranges = slices(u)
+                    check_knn_rows(c2, oracle, pts, 16, ranges)
+                    with native.Context() as t:
+                        t.build(*synth.precision_mix(2_000_000, 101))
+                        rep_l = learned.train_radius_model(t, 16, steps=600)
+                        c2.mlp_params(t.mlp_params())
+                    c2.mlp_set_margin(rep_l["margin"])
+                    c2.set_learned(True, skip_seed=True)
+                    check_knn_rows(c2, oracle, pts, 16, ranges)
+                    assert np.array_equal(c2.normals(16), nrm)
+                    report["learned_misses"] = c2.stats()["learned_misses"]
             ang = angle_deg_free(nrm[q], ref)
             rep = {"fp64_solves": fp64, "fp64_fraction": fp64 / u}
             for name, m in classes.items():
