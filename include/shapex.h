@@ -21,7 +21,7 @@
 extern "C" {
 #endif
 
-#define SE_ABI_VERSION 1
+#define SE_ABI_VERSION 2 /* 2: se_options and se_stats gained the cell-scan fields */
 
 /* The library exports exactly the functions below; everything else in it is
  * hidden. */
@@ -89,7 +89,16 @@ typedef struct se_options {
                                  2^22 polls; > 0: after this many */
     int32_t debug_inject;     /* SE_DEBUG_* bits; each fires once, on the next call
                                  that reaches it, and is then cleared */
-    int32_t reserved[1];
+    int32_t learned_cell_scan; /* with learned and learned_skip_seed: 1 runs the learned
+                                  attempt as a direct scan of the Morton cells that cover
+                                  each query's predicted ball (no tree walk; warps whose
+                                  cells are too many walk the tree); 0 (the default) walks
+                                  the tree with the predicted bound as a cap, which
+                                  measured faster on every cloud tried */
+    int32_t cell_span;         /* cell scan: at most this many cells per axis cover one
+                                  query's predicted ball (2..4; 0: the default, 3) */
+    int32_t cell_max_points;   /* cell scan: a warp whose cells hold more points walks the
+                                  tree instead (0: the default, 4096) */
 } se_options;
 
 /* se_options.debug_inject bits. */
@@ -217,6 +226,10 @@ typedef struct se_stats {
     int64_t merge_steps;     /* candidate-buffer merge steps, summed over warps */
     int64_t inserts;         /* insertions into the k-best lists, summed over queries */
     int64_t learned_misses;  /* queries whose learned radius was too small (searched again) */
+    int64_t cell_warps;      /* warps whose learned attempt scanned Morton cells (no tree walk) */
+    int64_t cell_fallbacks;  /* warps whose cells were too many: the learned attempt walked the tree */
+    int64_t cell_lookups;    /* cells whose code range was looked up, summed over warps */
+    int64_t cell_points;     /* points in the cells a warp scanned, summed over warps */
 } se_stats;
 SE_API int se_get_stats(const se_ctx* ctx, se_stats* stats);
 

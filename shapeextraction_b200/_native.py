@@ -52,7 +52,8 @@ class SeOptions(ctypes.Structure):
         ("device", ctypes.c_int32), ("stream", ctypes.c_void_p), ("seed_halo", ctypes.c_int32),
         ("learned", ctypes.c_int32), ("learned_skip_seed", ctypes.c_int32), ("search_compat", ctypes.c_int32),
         ("batch_graph", ctypes.c_int32), ("debug_wait_limit", ctypes.c_int32),
-        ("debug_inject", ctypes.c_int32), ("reserved", ctypes.c_int32 * 1),
+        ("debug_inject", ctypes.c_int32), ("learned_cell_scan", ctypes.c_int32),
+        ("cell_span", ctypes.c_int32), ("cell_max_points", ctypes.c_int32),
     ]
 
 
@@ -70,7 +71,7 @@ class SeDeviceViews(ctypes.Structure):
 
 
 STAT_NAMES = ["fp64_solves", "nodes_visited", "buckets_scanned", "candidates", "merge_steps", "inserts",
-              "learned_misses"]
+              "learned_misses", "cell_warps", "cell_fallbacks", "cell_lookups", "cell_points"]
 
 
 class SeStats(ctypes.Structure):
@@ -168,7 +169,7 @@ class Context:
     def __init__(self, code_bits=63, root_compat=True, build_octree=True, viewpoint=(0.0, 0.0, 0.0),
                  eigengap_fp64=1e-4, leaf_bucket=96, device=0, stream=None, seed_halo=-1, learned=False,
                  learned_skip_seed=False, search_compat=False, batch_graph=True, debug_wait_limit=0,
-                 debug_inject=0):
+                 debug_inject=0, learned_cell_scan=False, cell_span=0, cell_max_points=0):
         L = lib()
         o = SeOptions()
         L.se_options_init(ctypes.byref(o))
@@ -188,6 +189,9 @@ class Context:
         o.batch_graph = int(bool(batch_graph))
         o.debug_wait_limit = int(debug_wait_limit)
         o.debug_inject = int(debug_inject)
+        o.learned_cell_scan = int(bool(learned_cell_scan))
+        o.cell_span = int(cell_span)
+        o.cell_max_points = int(cell_max_points)
         self.options = o
         h = ctypes.c_void_p()
         rc = L.se_create(ctypes.byref(h), ctypes.byref(o))

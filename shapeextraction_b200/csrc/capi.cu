@@ -178,6 +178,31 @@ int run_query(se_ctx* c, int k, int64_t start, int64_t count, const float* ext, 
     }
     q.learned_r2 = use_learned ? c->r2_buf : nullptr;
     q.learned_skip_seed = c->opt.learned_skip_seed;
+    // with learned_cell_scan the learned attempt scans Morton cells directly
+    // (no tree walk); it needs the seed skipped
+    const bool cells = use_learned && c->opt.learned_skip_seed && c->opt.learned_cell_scan;
+    bool lut_launched = false;
+    if (cells && c->lut_level == 0) {
+        // table level: at least 2 codes per entry on average, 8^7 entries (8 MB) at most
+        const int bpa = c->opt.code_bits / 3;
+        int level = 1;
+        while (level < bpa && level < 7 && ((int64_t)8 << (3 * level)) * 2 <= u) ++level;
+        const int64_t n_ent = ((int64_t)1 << (3 * level)) + 1;
+        if (c->lut_cap < n_ent) {
+            SE_CUDA(c, regrow(c->lut_buf, n_ent), "alloc cell table");
+            c->lut_cap = n_ent;
+        }
+        SE_CUDA(c, enqueue_cell_lut(c->b, c->opt.code_bits, level, c->lut_buf, c->stream, c->num_sms),
+                "launch cell table");
+        c->lut_level = level;
+        lut_launched = true;
+    }
+    if (cells) {
+        q.cell_lut = c->lut_buf;
+        q.lut_shift = c->opt.code_bits / 3 - c->lut_level;
+        q.cell_pmax = c->opt.cell_max_points > 0 ? c->opt.cell_max_points : 4096;
+        q.cell_span = c->opt.cell_span > 0 ? c->opt.cell_span : 3;
+    }
     const bool host = mem == SE_MEM_HOST;
     if (ext) {
         if (host) {
@@ -255,7 +280,7 @@ int run_query(se_ctx* c, int k, int64_t start, int64_t count, const float* ext, 
                                        c->stream),
                     "copy normals");
     }
-    c->query_launches = use_learned ? 2 : 1;
+    c->query_launches = (use_learned ? 2 : 1) + (lut_launched ? 1 : 0);
     c->have_query_times = true;
     SE_CUDA(c, cudaMemcpyAsync(&c->h_st->err, &c->b.st->err, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream),
             "read state");
@@ -320,6 +345,9 @@ int se_create(se_ctx** out, const se_options* opt) {
     if (o.seed_halo > 48) return SE_ERR_INVALID_ARG;
     if (!(o.eigengap_fp64 >= 0.0f)) return SE_ERR_INVALID_ARG;
     if (o.debug_wait_limit < 0) return SE_ERR_INVALID_ARG;
+    if (o.learned_cell_scan != 0 && o.learned_cell_scan != 1) return SE_ERR_INVALID_ARG;
+    if (o.cell_span != 0 && (o.cell_span < 2 || o.cell_span > 4)) return SE_ERR_INVALID_ARG;
+    if (o.cell_max_points < 0) return SE_ERR_INVALID_ARG;
     if (o.debug_inject & ~(SE_DEBUG_STALL_SORT_TILE | SE_DEBUG_SEARCH_LIMIT | SE_DEBUG_ALLOC_FAIL))
         return SE_ERR_INVALID_ARG;
     se_ctx* c = new se_ctx();
@@ -374,6 +402,7 @@ int se_destroy(se_ctx* c) {
                          c->mw.yhat, c->mw.h1, c->mw.h2, c->mw.dy, c->mw.dh1, c->mw.dh2};
     for (float* p : mlp_bufs)
         if (p) cudaFree(p);
+    if (c->lut_buf) cudaFree(c->lut_buf);
     for (BatchLane& l : c->lanes) {
         if (l.stream) cudaStreamSynchronize(l.stream);
         void* ptrs[] = {l.b.keys0, l.b.keys1, l.b.lookback, l.b.lookback64, l.b.codes, l.b.pts4, l.b.pts3,
@@ -418,6 +447,7 @@ int se_build(se_ctx* c, const float* x, const float* y, const float* z, int64_t 
     NvtxRange nvtx("shapex.se_build");
     if (int rc = prologue(c)) return rc;
     c->built = false;
+    c->lut_level = 0;
     if (int rc = check_mem(c, mem)) return rc;
     if (n < 0) return fail(c, SE_ERR_INVALID_ARG, "negative point count");
     if (n > ((int64_t)1 << 30) - 1) return fail(c, SE_ERR_INVALID_ARG, "more than 2^30 - 1 points");

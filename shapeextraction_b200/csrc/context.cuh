@@ -76,6 +76,10 @@ struct se_ctx {
     int64_t mw_cap = 0;
     float* r2_buf = nullptr;
     int64_t r2_cap = 0;
+    // code-range table of the current build for the learned cell scan
+    uint32_t* lut_buf = nullptr;
+    int64_t lut_cap = 0;
+    int lut_level = 0;  // 0: not built for the current build
     float* xs_buf = nullptr;  // staging of host features / targets / outputs
     int64_t xs_cap = 0;
 

@@ -159,10 +159,15 @@ struct QArgs {
     int learned_skip_seed;
     int device_count;  // 1: u = count = the build's unique-point count, read on the device (start 0)
     int step_limit;    // > 0: node visits per warp before the walk gives up (test hook)
+    const uint32_t* cell_lut;  // learned cell scan: code-range table (null: tree walk with the cap)
+    int lut_shift;             // per-axis shift of the table's level (bits per axis - level)
+    int cell_pmax;             // cell scan: most points per warp before it falls back to the walk
+    int cell_span;             // cell scan: most cells per axis covering one lane's ball (2..4)
 };
 
 struct Counters {
-    int cand = 0, ins = 0, merge = 0, buckets = 0, lmiss = 0;
+    int cand = 0, ins = 0, merge = 0, buckets = 0, lmiss = 0, cells = 0, cell_fallback = 0, cell_lookups = 0,
+        cell_points = 0;
 };
 
 // Merge every lane's buffered candidates into its list; the warp steps
@@ -263,6 +268,272 @@ __device__ __forceinline__ void scan_sparse(int32_t first, int cnt, uint32_t mas
     __syncwarp();
 }
 
+// Position of set bit number n (from 0) of w; w has more than n set bits.
+__device__ __forceinline__ int nth_set_bit(uint32_t w, int n) {
+    int pos = 0;
+#pragma unroll
+    for (int width = 16; width >= 1; width >>= 1) {
+        const int c = __popc(w & ((1u << width) - 1u));
+        if (n >= c) {
+            n -= c;
+            w >>= width;
+            pos += width;
+        }
+    }
+    return pos;
+}
+
+// First index in codes[lo, hi) whose code is >= key (hi when none).
+__device__ __forceinline__ uint32_t lower_bound_codes(const uint64_t* __restrict__ codes, uint32_t lo, uint32_t hi,
+                                                      uint64_t key) {
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(codes + mid) < key) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Bounds of the decoded coordinates X0..X1 of one axis, for pruning: the
+// decode (codeToPoint: fma(X / M, range, min)) is evaluated with a multiply by
+// 1/M instead of the division and widened by `pad`, which exceeds the
+// difference between the two evaluations (at most range * 2^-22 + max|coord| *
+// 2^-23), so every decoded point of the range lies inside [lo, hi].
+__device__ __forceinline__ void axis_bounds(uint32_t X0, uint32_t X1, float inv_m, float mn, float range, float pad,
+                                            float& lo, float& hi) {
+    lo = __fmaf_rn((float)X0 * inv_m, range, mn) - pad;
+    hi = __fmaf_rn((float)X1 * inv_m, range, mn) + pad;
+}
+
+constexpr int kCellBits = 1024;   // cells of a warp's union grid: one bit each, in stack[0, 32)
+constexpr int kCellRanges = 64;   // nonempty cells a warp scans: listed in pts[32, 96), order keys after
+
+// Learned attempt as a direct scan of Morton cells, with no tree walk.
+//
+// Each lane's predicted ball (radius sqrt(cap) around its query) is covered by
+// an integer box of code coordinates, widened by the decode rounding, and the
+// warp picks the finest level at which every lane's box spans at most
+// cell_span cells per axis. The union of the lanes' cells is marked in a
+// shared bitmap; each marked cell is the contiguous run of sorted codes under
+// its prefix, found with the build's code-range table and a short binary
+// search. The nonempty cells are taken nearest first (box distance to the
+// warp's first query); a cell that no lane's current bound reaches any more is
+// skipped, and the points of the others are packed into 32-point chunks that
+// every lane tests against its own bound (dense: no per-lane loops). Every
+// point within a lane's cap lies in one of its cells and is offered to it
+// unless the lane's bound already excludes the cell's box, so a lane whose
+// k-th distance ends within its cap has its exact k best; the caller searches
+// the others again. Returns false, having offered nothing, when the warp's
+// cells are too many (queries spread across distant regions) or hold more
+// than cell_pmax points; the caller then walks the tree with the cap.
+template <int K, bool EXACT, class WS>
+__device__ __forceinline__ bool cell_scan(TopK<K, EXACT>& tk, int& bc, WS& W, int lane, Counters& ct,
+                                          const float4* __restrict__ pts, const uint64_t* __restrict__ codes,
+                                          const QArgs& a, const DevState* st, bool act, int64_t qi, float qx,
+                                          float qy, float qz, float cap) {
+    constexpr int kBuf = KnnCfg<K>::buf;
+    const int bpa = a.code_bits / 3;
+    const uint32_t M = bitscale_of(a.code_bits);
+    const float fbs = (float)M;
+    const float mn = st->min_coord, range = st->range;
+    const bool ok = act && cap >= 0.0f && cap < INFINITY;  // false for NaN
+    uint32_t lo[3] = {0u, 0u, 0u}, hi[3] = {0u, 0u, 0u};
+    int s = 0;
+    if (ok) {
+        // |x_p - x_q| <= R for every point within the cap (dist2's rounding
+        // costs far less than the 1e-6 added); in code units the decode adds
+        // at most 1/4 + 2^-23 * M * max|coordinate| / range on each side.
+        const float R = __fmul_ru(__fsqrt_ru(cap), 1.000001f);
+        const float ru = __fmul_ru(R, __fdiv_ru(fbs, range));
+        const float big = fmaxf(fabsf(mn), fabsf(mn + range));
+        const float slack = __fadd_ru(__fmul_ru(__fmul_ru(1.1920929e-7f, fbs), __fdiv_ru(big, range)), 0.25f);
+        const float ext = __fadd_ru(ru, slack) + 1.0f;
+        const int64_t e = ext < 4.0e9f ? (int64_t)ceilf(ext) : ((int64_t)1 << 40);  // NaN range: whole cube
+        const uint64_t code = __ldg(codes + qi);
+        uint32_t dmax = 0;
+#pragma unroll
+        for (int ax = 0; ax < 3; ++ax) {
+            const int64_t X = (int64_t)gather3(code >> ax);
+            lo[ax] = (uint32_t)max64(0, X - e);
+            hi[ax] = (uint32_t)min64((int64_t)M, X + e);
+            dmax = max(dmax, hi[ax] - lo[ax]);
+        }
+        // the finest level at which the box spans at most cell_span cells per
+        // axis: (hi >> s) - (lo >> s) <= (dmax >> s) + 1 <= cell_span - 1
+        while ((int)(dmax >> s) > a.cell_span - 2) ++s;
+    }
+    const uint32_t okm = __ballot_sync(FULL, ok);
+    if (!okm) return true;  // no lane has a usable cap: every active lane is searched again
+    s = (int)__reduce_max_sync(FULL, (unsigned)(ok ? s : 0));
+    uint32_t A[3], g[3];
+    for (int tries = 0;; ++tries) {
+        uint64_t cells = 1;
+#pragma unroll
+        for (int ax = 0; ax < 3; ++ax) {
+            A[ax] = __reduce_min_sync(FULL, ok ? (lo[ax] >> s) : 0xffffffffu);
+            const uint32_t b = __reduce_max_sync(FULL, ok ? (hi[ax] >> s) : 0u);
+            g[ax] = b - A[ax] + 1;
+            cells *= g[ax];
+        }
+        if (cells <= (uint64_t)kCellBits) break;
+        if (tries == 2 || s >= bpa) {
+            ++ct.cell_fallback;
+            return false;
+        }
+        ++s;
+    }
+    // mark the union of the lanes' cells
+    uint32_t* bits = reinterpret_cast<uint32_t*>(W.stack);  // words [0, 32); inclusive prefixes at [32, 64)
+    __syncwarp();
+    bits[lane] = 0u;
+    __syncwarp();
+    if (ok) {
+        for (uint32_t z = (lo[2] >> s) - A[2]; z <= (hi[2] >> s) - A[2]; ++z)
+            for (uint32_t y = (lo[1] >> s) - A[1]; y <= (hi[1] >> s) - A[1]; ++y)
+                for (uint32_t x = (lo[0] >> s) - A[0]; x <= (hi[0] >> s) - A[0]; ++x) {
+                    const uint32_t b = (z * g[1] + y) * g[0] + x;
+                    atomicOr(&bits[b >> 5], 1u << (b & 31));
+                }
+    }
+    __syncwarp();
+    const uint32_t word = bits[lane];
+    int incl = __popc(word);
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += t;
+    }
+    const int total = __shfl_sync(FULL, incl, 31);
+    uint32_t* pre = bits + 32;
+    pre[lane] = (uint32_t)incl;
+    __syncwarp();
+    // one cell per lane per round: its code range and its order key
+    int4* list = reinterpret_cast<int4*>(&W.pts[32]);                         // (first, count, prefix lo, hi)
+    uint32_t* okeys = reinterpret_cast<uint32_t*>(&W.pts[32 + kCellRanges]);  // scan order keys
+    const uint32_t* lut = a.cell_lut;
+    const int ls = a.lut_shift;
+    const float inv_m = 1.0f / fbs;
+    const float big = fmaxf(fabsf(mn), fabsf(mn + range));
+    const float pad = __fadd_ru(__fmul_ru(big, 4.76837158e-7f), __fmul_ru(range, 9.53674316e-7f));  // 2^-21, 2^-20
+    // order reference: the warp's first query with a usable cap
+    const int ref = __ffs(okm) - 1;
+    const float rx = __shfl_sync(FULL, qx, ref), ry = __shfl_sync(FULL, qy, ref), rz = __shfl_sync(FULL, qz, ref);
+    int nr = 0;
+    int64_t ptotal = 0;
+    ct.cell_lookups += total;
+    for (int r0 = 0; r0 < total; r0 += 32) {
+        const int idx = r0 + lane;
+        uint32_t first = 0, cnt = 0;
+        uint64_t P = 0;
+        float key = 0.0f;
+        if (idx < total) {
+            int w = 0;  // the word holding marked cell number idx
+#pragma unroll
+            for (int step = 16; step >= 1; step >>= 1)
+                if ((int)pre[w + step - 1] <= idx) w += step;
+            const int before = w > 0 ? (int)pre[w - 1] : 0;
+            const uint32_t b = (uint32_t)(w * 32 + nth_set_bit(bits[w], idx - before));
+            const uint32_t C[3] = {A[0] + b % g[0], A[1] + (b / g[0]) % g[1], A[2] + b / (g[0] * g[1])};
+            P = spread3(C[0]) | (spread3(C[1]) << 1) | (spread3(C[2]) << 2);
+            uint32_t last;
+            if (s >= ls) {
+                const int d = 3 * (s - ls);
+                first = __ldg(lut + (P << d));
+                last = __ldg(lut + ((P + 1) << d));
+            } else {
+                const uint64_t j = P >> (3 * (ls - s));
+                const uint32_t l0 = __ldg(lut + j), l1 = __ldg(lut + j + 1);
+                first = lower_bound_codes(codes, l0, l1, P << (3 * s));
+                last = lower_bound_codes(codes, first, l1, (P + 1) << (3 * s));
+            }
+            cnt = last - first;
+            float bl[3], bh[3];
+#pragma unroll
+            for (int ax = 0; ax < 3; ++ax)
+                axis_bounds(C[ax] << s, (uint32_t)min64((int64_t)M, ((int64_t)(C[ax] + 1) << s) - 1), inv_m, mn, range,
+                            pad, bl[ax], bh[ax]);
+            key = box_dist2(rx, ry, rz, bl[0], bl[1], bl[2], bh[0], bh[1], bh[2]);
+        }
+        const bool keep = cnt > 0;
+        const uint32_t km = __ballot_sync(FULL, keep);
+        if (keep) {
+            const int pos = nr + __popc(km & lanemask_lt());
+            if (pos < kCellRanges) {
+                list[pos] = make_int4((int)first, (int)cnt, (int)(uint32_t)P, (int)(uint32_t)(P >> 32));
+                okeys[pos] = (__float_as_uint(key) & ~0x7fu) | (uint32_t)pos;  // distance bits, entry number
+            }
+        }
+        nr += __popc(km);
+        ptotal += (int64_t)__reduce_add_sync(FULL, keep ? min(cnt, 1u << 26) : 0u);
+    }
+    if (nr > kCellRanges || ptotal > (int64_t)a.cell_pmax) {
+        ++ct.cell_fallback;
+        return false;
+    }
+    __syncwarp();
+    ++ct.cells;
+    ct.cell_points += (int)ptotal;
+    // Cells nearest first, so that the bounds tighten early. Lane l holds the
+    // order keys of entries l and l + 32. A cell goes on only if some lane's
+    // current bound (its k-th distance so far, at most its cap) reaches the
+    // cell's box; its points are appended to the staging chunk pts[0, 32)
+    // (index in .w), and each full chunk is tested by every lane.
+    uint32_t ok0 = lane < nr ? okeys[lane] : 0xffffffffu;
+    uint32_t ok1 = lane + 32 < nr ? okeys[lane + 32] : 0xffffffffu;
+    int fill = 0;
+    bool merged = false;
+    auto test_chunk = [&](int n) {
+        __syncwarp();
+        if (__any_sync(FULL, bc + n > kBuf)) flush(tk, bc, W, lane, ct, pts, qx, qy, qz);
+        if (ok) {
+            const float b2 = fminf(tk.tau(), cap);
+            for (int t = 0; t < n; ++t) {
+                const float4 p = W.pts[t];
+                if (dist2(qx, qy, qz, p.x, p.y, p.z) <= b2) W.buf[bc++][lane] = __float_as_int(p.w);
+            }
+        }
+        __syncwarp();
+        if (!merged) {  // the nearest points usually hold most of each list: merge them at once
+            merged = true;
+            flush(tk, bc, W, lane, ct, pts, qx, qy, qz);
+        }
+    };
+    for (int it = 0; it < nr; ++it) {
+        const uint32_t m = __reduce_min_sync(FULL, min(ok0, ok1));
+        if (ok0 == m) ok0 = 0xffffffffu;
+        if (ok1 == m) ok1 = 0xffffffffu;
+        const int4 r = list[m & 0x7fu];
+        const uint64_t P = (uint64_t)(uint32_t)r.z | ((uint64_t)(uint32_t)r.w << 32);
+        float bl[3], bh[3];
+#pragma unroll
+        for (int ax = 0; ax < 3; ++ax) {
+            const uint32_t Cax = gather3(P >> ax);
+            axis_bounds(Cax << s, (uint32_t)min64((int64_t)M, ((int64_t)(Cax + 1) << s) - 1), inv_m, mn, range, pad,
+                        bl[ax], bh[ax]);
+        }
+        const bool need = ok && box_dist2(qx, qy, qz, bl[0], bl[1], bl[2], bh[0], bh[1], bh[2]) <= fminf(tk.tau(), cap);
+        if (!__any_sync(FULL, need)) continue;
+        ++ct.buckets;
+        for (int off = 0; off < r.y;) {
+            const int take = min(r.y - off, 32 - fill);
+            if (lane < take) {
+                const int32_t pi = r.x + off + lane;
+                float4 p = __ldg(pts + pi);
+                p.w = __int_as_float(pi);
+                W.pts[fill + lane] = p;
+            }
+            fill += take;
+            off += take;
+            if (fill == 32) {
+                test_chunk(32);
+                fill = 0;
+            }
+        }
+    }
+    if (fill > 0) test_chunk(fill);
+    return true;
+}
+
 __device__ __forceinline__ void neu_add(float& s, float& c, float x) {
     const float t = s + x;
     if (fabsf(s) >= fabsf(x)) c += (s - t) + x;
@@ -348,7 +619,10 @@ __device__ __forceinline__ void estimate_normal(const int32_t* nbr, int k, const
 }
 
 // The 32 queries [q0, q0 + 32) of one warp: search, then the outputs.
-template <int K, bool EXACT, bool EXT, bool NORMALS>
+// CELLS: the learned attempt may run the cell scan (a separate instantiation,
+// launched only when the caller turned the cell scan on: compiled into the
+// default kernels, its code alone slowed them by about 8%).
+template <int K, bool EXACT, bool EXT, bool NORMALS, bool CELLS>
 __device__ __forceinline__ void knn_warp(const float4* __restrict__ pts, const SNode* __restrict__ snodes,
                                          const uint64_t* __restrict__ codes, const QArgs& a, DevState* st,
                                          int64_t q0, WarpSmem<KnnCfg<K>::buf>& W, int lane) {
@@ -408,6 +682,11 @@ __device__ __forceinline__ void knn_warp(const float4* __restrict__ pts, const S
         const int64_t sw0 = seed ? w0 : 0, sw1 = seed ? w1 : 0;  // points offered by the seed
         if (act) tk.init(a.k);
         int bc = 0;  // buffered candidates of this lane
+        // learned attempt as a cell scan (falls back to the capped tree walk)
+        const bool scanned = CELLS && attempt == 0 && a.cell_lut != nullptr &&
+                             cell_scan<K, EXACT>(tk, bc, W, lane, ct, pts, codes, a, st, act,
+                                                 a.start + (active ? qo : q0), qx, qy, qz, cap);
+        __syncwarp();
         if (seed) {
             // Seed: each lane walks the Morton window outwards from its own
             // position (0, +1, -1, +2, ...), so its first candidates are its
@@ -452,7 +731,7 @@ __device__ __forceinline__ void knn_warp(const float4* __restrict__ pts, const S
             } while (t < nsteps);
         }
 
-        if (u >= 2 && (sw0 > 0 || sw1 < u)) {
+        if (!scanned && u >= 2 && (sw0 > 0 || sw1 < u)) {
             int sp = 1;
             if (lane == 0) W.stack[0] = 0;
             __syncwarp();
@@ -532,7 +811,10 @@ __device__ __forceinline__ void knn_warp(const float4* __restrict__ pts, const S
         }
         flush(tk, bc, W, lane, ct, pts, qx, qy, qz);
         if (attempt == 0) {
-            const bool miss = act && !(tk.tau() <= cap);
+            // a lane the cell scan could not serve (its cap is +inf or not a
+            // number) was offered nothing: search it again as a miss
+            const bool unserved = scanned && !(cap >= 0.0f && cap < INFINITY);
+            const bool miss = act && (unserved || !(tk.tau() <= cap));
             ct.lmiss += miss;
             act = miss;
             if (!__any_sync(FULL, act)) break;
@@ -543,6 +825,10 @@ __device__ __forceinline__ void knn_warp(const float4* __restrict__ pts, const S
         const unsigned ins = __reduce_add_sync(FULL, (unsigned)ct.ins);
         const unsigned lmiss = __reduce_add_sync(FULL, (unsigned)ct.lmiss);
         if (lane == 0) {
+            if (ct.cells) atomicAdd(&st->counters[CNT_CELL_WARPS], (unsigned long long)ct.cells);
+            if (ct.cell_fallback) atomicAdd(&st->counters[CNT_CELL_FALLBACK], (unsigned long long)ct.cell_fallback);
+            if (ct.cell_lookups) atomicAdd(&st->counters[CNT_CELL_LOOKUPS], (unsigned long long)ct.cell_lookups);
+            if (ct.cell_points) atomicAdd(&st->counters[CNT_CELL_POINTS], (unsigned long long)ct.cell_points);
             atomicAdd(&st->counters[CNT_NODES], (unsigned long long)steps);
             atomicAdd(&st->counters[CNT_BUCKETS], (unsigned long long)ct.buckets);
             atomicAdd(&st->counters[CNT_MERGE], (unsigned long long)ct.merge);
@@ -579,7 +865,7 @@ __device__ __forceinline__ void knn_warp(const float4* __restrict__ pts, const S
     }
 }
 
-template <int K, bool EXACT, bool EXT, bool NORMALS>
+template <int K, bool EXACT, bool EXT, bool NORMALS, bool CELLS>
 __global__ void __launch_bounds__(KnnCfg<K>::threads, KnnCfg<K>::min_blocks)
     k_knn(const float4* __restrict__ pts, const SNode* __restrict__ snodes,
                                                      const uint64_t* __restrict__ codes, QArgs a, DevState* st) {
@@ -588,7 +874,7 @@ __global__ void __launch_bounds__(KnnCfg<K>::threads, KnnCfg<K>::min_blocks)
     using WS = WarpSmem<KnnCfg<K>::buf>;
     WS& W = reinterpret_cast<WS*>(knn_smem)[warp];
     const int64_t q0 = ((int64_t)blockIdx.x * KnnCfg<K>::warps + warp) * 32;
-    knn_warp<K, EXACT, EXT, NORMALS>(pts, snodes, codes, a, st, q0, W, lane);
+    knn_warp<K, EXACT, EXT, NORMALS, CELLS>(pts, snodes, codes, a, st, q0, W, lane);
 }
 
 // Persistent kernel over many clouds that share k: each warp takes the next
@@ -620,18 +906,20 @@ __global__ void __launch_bounds__(KnnCfg<K>::threads, KnnCfg<K>::min_blocks)
         ca.out_normals = d.out_normals;
         ca.start = 0;
         ca.device_count = 1;
-        knn_warp<K, EXACT, false, true>(d.pts, d.snodes, nullptr, ca, d.st, ((int64_t)item - d.item0) * 32, W, lane);
+        knn_warp<K, EXACT, false, true, false>(d.pts, d.snodes, nullptr, ca, d.st, ((int64_t)item - d.item0) * 32, W,
+                                               lane);
         __syncwarp();
     }
 }
 
-template <int K, bool EXACT, bool EXT, bool NORMALS>
+template <int K, bool EXACT, bool EXT, bool NORMALS, bool CELLS = false>
 cudaError_t launch_one(const BuildBufs& b, const QArgs& a, unsigned blocks, cudaStream_t s) {
     constexpr int smem = (int)sizeof(WarpSmem<KnnCfg<K>::buf>) * KnnCfg<K>::warps;
-    cudaError_t e =
-        cudaFuncSetAttribute(k_knn<K, EXACT, EXT, NORMALS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaError_t e = cudaFuncSetAttribute(k_knn<K, EXACT, EXT, NORMALS, CELLS>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    k_knn<K, EXACT, EXT, NORMALS><<<blocks, KnnCfg<K>::threads, smem, s>>>(b.pts4, b.snodes, b.codes, a, b.st);
+    k_knn<K, EXACT, EXT, NORMALS, CELLS><<<blocks, KnnCfg<K>::threads, smem, s>>>(b.pts4, b.snodes, b.codes, a,
+                                                                                   b.st);
     return cudaGetLastError();
 }
 
@@ -640,6 +928,10 @@ cudaError_t launch_k(const BuildBufs& b, const QArgs& a, bool ext, bool normals,
     const int64_t warps = (a.count + 31) / 32;
     const unsigned blocks = (unsigned)((warps + KnnCfg<K>::warps - 1) / KnnCfg<K>::warps);
     if (ext) return launch_one<K, EXACT, true, false>(b, a, blocks, s);
+    if (a.cell_lut) {
+        if (normals) return launch_one<K, EXACT, false, true, true>(b, a, blocks, s);
+        return launch_one<K, EXACT, false, false, true>(b, a, blocks, s);
+    }
     if (normals) return launch_one<K, EXACT, false, true>(b, a, blocks, s);
     return launch_one<K, EXACT, false, false>(b, a, blocks, s);
 }
@@ -662,7 +954,29 @@ cudaError_t launch_batch(const BatchCloud* clouds, int n_clouds, int64_t n_items
     return cudaGetLastError();
 }
 
+// lut[j] = lower bound of j << sh in the u sorted unique codes, for j in
+// [0, n_ent]; the code count u is read on the device from the build state.
+__global__ void __launch_bounds__(256) k_cell_lut(const uint64_t* __restrict__ codes, const DevState* st, int sh,
+                                                  int64_t n_ent, uint32_t* __restrict__ lut) {
+    const uint32_t u = (uint32_t)st->u;
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j <= n_ent;
+         j += (int64_t)gridDim.x * blockDim.x) {
+        lut[j] = j == n_ent ? u : lower_bound_codes(codes, 0u, u, (uint64_t)j << sh);
+    }
+}
+
 }  // namespace
+
+cudaError_t enqueue_cell_lut(const BuildBufs& b, int code_bits, int level, uint32_t* lut, cudaStream_t s,
+                             int num_sms) {
+    const int bpa = code_bits / 3;
+    if (level < 1 || level > bpa || level > 10) return cudaErrorInvalidValue;
+    const int64_t n_ent = (int64_t)1 << (3 * level);
+    const int64_t want = (n_ent + 256) / 256;
+    const unsigned blocks = (unsigned)(want < (int64_t)num_sms * 16 ? want : (int64_t)num_sms * 16);
+    k_cell_lut<<<blocks, 256, 0, s>>>(b.codes, b.st, 3 * (bpa - level), n_ent, lut);
+    return cudaGetLastError();
+}
 
 __global__ void k_batch_collect(const DevState* __restrict__ st, int n, unsigned long long* __restrict__ u_out,
                                 uint32_t* __restrict__ err_out) {
@@ -732,6 +1046,10 @@ cudaError_t enqueue_query(const BuildBufs& b, const QueryParams& q, cudaStream_t
     a.learned_skip_seed = q.learned_skip_seed;
     a.device_count = q.device_count;
     a.step_limit = q.step_limit;
+    a.cell_lut = q.learned_r2 ? q.cell_lut : nullptr;
+    a.lut_shift = q.lut_shift;
+    a.cell_pmax = q.cell_pmax;
+    a.cell_span = q.cell_span < 2 ? 2 : (q.cell_span > 4 ? 4 : q.cell_span);
     if (a.seed_halo > kMaxHalo) a.seed_halo = kMaxHalo;
     if (a.seed_halo < 0) a.seed_halo = 0;
     const bool ext = q.ext_queries != nullptr;

@@ -22,7 +22,7 @@ constexpr int kScanTile = kScanThreads * kScanIpt;
 // Query counters: fp64 solves, nodes visited, buckets scanned, candidates,
 // merge steps, inserts.
 enum { CNT_FP64 = 0, CNT_NODES, CNT_BUCKETS, CNT_CANDIDATES, CNT_MERGE, CNT_INSERTS, CNT_LEARNED_MISS,
-       kQueryCounters };
+       CNT_CELL_WARPS, CNT_CELL_FALLBACK, CNT_CELL_LOOKUPS, CNT_CELL_POINTS, kQueryCounters };
 
 // Small device-resident state of one build (zeroed at the start of each build).
 struct DevState {
@@ -184,7 +184,20 @@ struct QueryParams {
     int compat;               // 1: the reference's approximate octree search and FP32 covariance
     int64_t n_octree;         // octree nodes (compat search)
     int step_limit = 0;       // > 0: node visits per warp before the walk gives up (test hook)
+    // learned cell scan: the code-range table of this build (null: the learned
+    // attempt walks the tree with the cap), its per-axis shift, and the most
+    // points a warp scans before it falls back to the walk
+    const uint32_t* cell_lut = nullptr;
+    int lut_shift = 0;
+    int cell_pmax = 0;
+    int cell_span = 3;
 };
+
+// Code-range table of a build for the learned cell scan: lut[j] = the number
+// of unique codes below j << (3 * (bits per axis - level)), j = 0 .. 8^level
+// (lut[8^level] = u). Level between 1 and the bits per axis.
+cudaError_t enqueue_cell_lut(const BuildBufs& b, int code_bits, int level, uint32_t* lut, cudaStream_t s,
+                             int num_sms);
 
 cudaError_t enqueue_query(const BuildBufs& b, const QueryParams& q, cudaStream_t s, int num_sms);
 

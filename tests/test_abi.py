@@ -44,8 +44,8 @@ def test_options_defaults(native):
     assert tuple(o.viewpoint) == (0.0, 0.0, 0.0)
     assert o.search_compat == 0 and o.learned == 0 and o.batch_graph == 1
     assert o.leaf_bucket == 96 and o.seed_halo == -1  # 96-point buckets; halo picked per k
-    assert ctypes.sizeof(o) == 80  # sizeof(se_options) in C: 17 four-byte fields, a pointer, 4 B padding
-    assert L.se_abi_version() == 1
+    assert ctypes.sizeof(o) == 88  # sizeof(se_options) in C: 19 four-byte fields, a pointer, 4 B padding
+    assert L.se_abi_version() == 2
     assert L.se_status_string(5) == b"SE_ERR_NONFINITE"
 
 

@@ -6,7 +6,7 @@ search (work counters)."""
 import numpy as np
 import pytest
 
-from shapeextraction_b200 import synth
+from shapeextraction_b200 import learned, synth
 
 
 def _rand_params(seed):
@@ -116,8 +116,65 @@ def test_learned_search_exact_and_gain(native, oracle, trained):
             s = c.stats()
             assert s["learned_misses"] < 0.05 * pts.shape[0]
             assert s["candidates"] < s_plain["candidates"]  # tighter starting bound
+            assert s["cell_warps"] == 0 and s["cell_fallbacks"] == 0  # the capped tree walk
         ei, ed = oracle.knn_exact(pts, pts[:20000], 16)
         assert np.array_equal(plain_idx[:20000], ei)
+    # the cell scan (the learned attempt without a tree walk) gives the same lists
+    with native.Context(learned_cell_scan=True) as c:
+        c.build(x, y, z)
+        learned.transfer(src, c, rep["margin"])
+        c.set_learned(True, skip_seed=True)
+        idx, d2 = c.knn_self(16, with_d2=True)
+        assert np.array_equal(idx, plain_idx) and np.array_equal(d2, plain_d2)
+        assert np.array_equal(c.normals(16), plain_n)
+        s = c.stats()
+        warps = (pts.shape[0] + 31) // 32
+        assert s["cell_warps"] > 0.9 * warps, s
+        assert s["cell_warps"] + s["cell_fallbacks"] == warps
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("k", [1, 5, 8, 10, 12, 16, 20, 32])
+def test_cell_scan_exact_on_lattice_ties(native, oracle, trained, k):
+    """Integer lattice with repeated points (many equal distances): the cell
+    scan offers candidates in another order than the walk, and the lists must
+    still equal the oracle's, ties broken by index. Every k's kernel runs the
+    cell scan (the model's bounds are per-cloud, so calibration does not
+    matter for exactness)."""
+    src, rep = trained
+    rng = np.random.default_rng(5)
+    x, y, z = (rng.integers(0, 40, 80_000).astype(np.float32) for _ in range(3))
+    with native.Context(learned_cell_scan=True) as c:
+        c.build(x, y, z)
+        learned.transfer(src, c, rep["margin"])
+        pts = c.points()
+        c.set_learned(True, skip_seed=True)
+        idx, d2 = c.knn_self(k, with_d2=True)
+        ei, ed = oracle.knn_exact(pts, pts, k)
+        assert np.array_equal(d2, ed)
+        assert np.array_equal(idx, ei)
+        assert c.stats()["cell_warps"] > 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("margin", [6.0, 40.0])
+def test_cell_scan_oversized_caps_fall_back_exactly(native, oracle, trained, margin):
+    """Caps far too large: the warps' cells hold more points than a cell scan
+    takes (or span the whole cube), so the learned attempt walks the tree with
+    the cap instead; results stay exact."""
+    src, rep = trained
+    x, y, z = synth.scene(60_000, 3)
+    with native.Context(learned_cell_scan=True) as c:
+        c.build(x, y, z)
+        c.mlp_params(src.mlp_params())
+        c.mlp_set_margin(margin)
+        c.set_learned(True, skip_seed=True)
+        idx, d2 = c.knn_self(16, with_d2=True)
+        s = c.stats()
+        assert s["cell_fallbacks"] > 0, s
+        pts = c.points()
+        ei, ed = oracle.knn_exact(pts, pts, 16)
+        assert np.array_equal(idx, ei) and np.array_equal(d2, ed)
 
 
 @pytest.mark.gpu
@@ -128,12 +185,20 @@ def test_learned_forced_misses_fall_back(native, oracle, trained):
         c.build(x, y, z)
         c.mlp_params(src.mlp_params())
         c.mlp_set_margin(-12.0)  # bounds far too small: every query misses
-        c.set_learned(True)
-        idx = c.knn_self(16)
-        assert c.stats()["learned_misses"] == c.info()["n_points"]
         pts = c.points()
         ei, _ = oracle.knn_exact(pts, pts, 16)
-        assert np.array_equal(idx, ei)
+        for skip in (False, True):  # the capped walk with and without the seed
+            c.set_learned(True, skip_seed=skip)
+            idx = c.knn_self(16)
+            assert c.stats()["learned_misses"] == c.info()["n_points"]
+            assert np.array_equal(idx, ei)
+    with native.Context(learned_cell_scan=True) as c:  # the cell scan
+        c.build(x, y, z)
+        c.mlp_params(src.mlp_params())
+        c.mlp_set_margin(-12.0)
+        c.set_learned(True, skip_seed=True)
+        assert np.array_equal(c.knn_self(16), ei)
+        assert c.stats()["learned_misses"] == c.info()["n_points"]
 
 
 @pytest.mark.gpu
