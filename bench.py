@@ -481,15 +481,15 @@ def run_batch(a):
     host = [torch.from_numpy(np.ascontiguousarray(np.concatenate([c[i] for c in clouds]), np.float32)).pin_memory()
             for i in range(3)]
     dev = [h.cuda() for h in host]
-    tuning = None
-    if a.autotune:
-        tuning = autotune.tune_batch(clouds, ks, device=local, cache_path=a.autotune_cache)
-        bucket, halo = tuning["leaf_bucket"], tuning["seed_halo"]
-    else:
-        bucket, halo = a.bucket, a.halo
     stream = torch.cuda.current_stream()
     ctx = Context(code_bits=wl["code_bits"], device=local, stream=stream.cuda_stream, eigengap_fp64=a.eigengap,
-                  leaf_bucket=bucket, seed_halo=halo)
+                  leaf_bucket=a.bucket, seed_halo=a.halo)
+    tuning = None
+    if a.autotune:
+        # the library's tuner on this batch (device-resident inputs), cached per class, set on ctx
+        tuning = autotune.tune_batch(tuple(dev), (ks, offsets), code_bits=wl["code_bits"], device=local,
+                                     cache_path=a.autotune_cache, ctx=ctx)
+    bucket, halo = ctx.batch_tuning()["leaf_bucket"], ctx.batch_tuning()["seed_halo"]
     out_dev = torch.empty((total, 3), dtype=torch.float32, device="cuda")
     out_host = torch.empty((total, 3), dtype=torch.float32).pin_memory()
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
@@ -548,6 +548,7 @@ def run_batch(a):
                        "unique_points": u_sum, "k_counts": {str(k): int((ks == k).sum()) for k in (8, 16, 32)},
                        "leaf_bucket": bucket,
                        "seed_halo": halo if halo >= 0 else "per k: 16 up to k=16, 32 above", "autotune": tuning,
+                       "batch_tuning": ctx.batch_tuning(),
                        "l2": "flushed by a 256 MB device write before every timed step",
                        "parallelism": f"{world} independent replica(s), one batch per GPU"},
             "e2e": {"value": u_all * a.steps / (ms_e2e * 1e-3), "unit": "normals/s", "ms_per_step": ms_e2e / a.steps,

@@ -99,6 +99,17 @@ typedef struct se_options {
                                   query's predicted ball (2..4; 0: the default, 3) */
     int32_t cell_max_points;   /* cell scan: a warp whose cells hold more points walks the
                                   tree instead (0: the default, 4096) */
+    /* se_normals_batch scheduling (0: the default of each); se_tune_batch
+     * measures and sets them, with leaf_bucket and seed_halo. */
+    int32_t batch_lanes;           /* streams the clouds' builds are spread over (1..16;
+                                      default 8) */
+    int32_t batch_lane_min_points; /* clouds of at least this many points are queried on
+                                      their stream right after their build, the others in
+                                      the shared persistent launches (default 65536) */
+    int32_t batch_blocks_per_sm;   /* resident blocks per SM of the persistent launches
+                                      (default: as many as fit) */
+    int32_t batch_warps_per_block; /* warps per block of the persistent launches: 2 or 4
+                                      (default: 4 up to k = 16, 2 above) */
 } se_options;
 
 /* se_options.debug_inject bits. */
@@ -216,6 +227,30 @@ SE_API int se_normals(se_ctx* ctx, int k, int64_t start, int64_t count, float* o
  * are host arrays; x, y, z and out_normals follow `mem`. */
 SE_API int se_normals_batch(se_ctx* ctx, const float* x, const float* y, const float* z, const int64_t* offsets,
                      int n_clouds, const int32_t* ks, float* out_normals, int64_t* out_u, int mem);
+
+/* Batch tuning: the bucket size, seed halo and scheduling that
+ * se_normals_batch uses (the options of the same names). No counterpart in
+ * the reference, which runs one cloud at a time and hard-codes 512 threads
+ * per block (src/CudaCommon.hpp:78). */
+typedef struct se_batch_tuning {
+    int32_t leaf_bucket;
+    int32_t seed_halo;
+    int32_t lanes;
+    int32_t lane_min_points;
+    int32_t blocks_per_sm;   /* 0: as many as fit */
+    int32_t warps_per_block; /* 0: per k */
+} se_batch_tuning;
+SE_API int se_get_batch_tuning(const se_ctx* ctx, se_batch_tuning* tuning);
+SE_API int se_set_batch_tuning(se_ctx* ctx, const se_batch_tuning* tuning);
+
+/* Autotuner for se_normals_batch: times the given batch (the same arguments
+ * as se_normals_batch, outputs to internal memory) with CUDA events under
+ * candidate tunings, one parameter at a time over two rounds (bucket 48..128,
+ * halo, lanes 4..16, lane cut-off 2^15..2^18, resident blocks, 2- or 4-warp
+ * blocks), `reps` timed calls each (median), and leaves the fastest set on
+ * the context. best and best_ms (optional) receive it and its time. */
+SE_API int se_tune_batch(se_ctx* ctx, const float* x, const float* y, const float* z, const int64_t* offsets,
+                  int n_clouds, const int32_t* ks, int mem, int reps, se_batch_tuning* best, float* best_ms);
 
 /* Work counters of the last se_normals/se_knn/se_knn_self call (diagnostics). */
 typedef struct se_stats {

@@ -881,6 +881,11 @@ int or_mlp_grad(const float* params, const float* X, const float* y, int64_t n, 
         loss += e * e / (double)n;
         const double dy = 2.0 * e / (double)n;
         g[B3] += dy;
+        // round_bf16 == 2 restates the tensor-core training step (k_mlp_train_tc):
+        // dh2 and dh1 enter the weight gradients, and dh2 the product that
+        // gives dh1, rounded to BF16; the bias gradients take them unrounded.
+        const bool tc = round_bf16 == 2;
+        auto rd = [&](double v) { return tc ? (double)bf16_round((float)v) : v; };
         double dh2[H], dh1[H];
         for (int i = 0; i < H; ++i) {
             g[W3 + i] += dy * h2[i];
@@ -890,14 +895,14 @@ int or_mlp_grad(const float* params, const float* X, const float* y, int64_t n, 
         for (int j = 0; j < H; ++j) {
             double a = 0.0;
             for (int i = 0; i < H; ++i) {
-                g[W2 + j * H + i] += h1[j] * dh2[i];
-                a += rw(W2 + j * H + i) * dh2[i];
+                g[W2 + j * H + i] += h1[j] * rd(dh2[i]);
+                a += rw(W2 + j * H + i) * rd(dh2[i]);
             }
             dh1[j] = h1[j] > 0 ? a : 0.0;
             g[B1 + j] += dh1[j];
         }
         for (int f = 0; f < F; ++f)
-            for (int i = 0; i < H; ++i) g[W1 + f * H + i] += x[f] * dh1[i];
+            for (int i = 0; i < H; ++i) g[W1 + f * H + i] += x[f] * rd(dh1[i]);
     }
     if (grads) std::copy(g.begin(), g.end(), grads);
     if (loss_out) *loss_out = loss;

@@ -212,7 +212,11 @@ MLP_PARAMS = 6337
 
 
 def mlp_grad(params, X, y, round_bf16=True):
-    """(yhat, loss, grads) of the learned-radius MLP's mean squared error."""
+    """(yhat, loss, grads) of the learned-radius MLP's mean squared error.
+    round_bf16: False (FP64 throughout), True (BF16 weights, inputs and
+    activations with FP32 accumulation, as the GPU's forward), or 2 (that,
+    plus the BF16 rounding of dh2 and dh1 that the tensor-core training step
+    applies before its products)."""
     params = _f32(params)
     X = _f32(X)
     y = _f32(y)
@@ -220,7 +224,8 @@ def mlp_grad(params, X, y, round_bf16=True):
     yhat = np.zeros(n, np.float64)
     grads = np.zeros(MLP_PARAMS, np.float64)
     loss = np.zeros(1, np.float64)
-    lib().or_mlp_grad(_p(params), _p(X), _p(y), n, int(bool(round_bf16)), _p(yhat), _p(grads), _p(loss))
+    mode = 2 if round_bf16 == 2 else int(bool(round_bf16))
+    lib().or_mlp_grad(_p(params), _p(X), _p(y), n, mode, _p(yhat), _p(grads), _p(loss))
     return yhat, float(loss[0]), grads
 
 

@@ -35,6 +35,7 @@ EXPORTS = [
     "se_get_points", "se_knn_self", "se_knn", "se_normals", "se_get_stats", "se_get_profile", "se_synchronize",
     "se_sort_keys_static", "se_features", "se_mlp_init", "se_mlp_params", "se_mlp_enable", "se_mlp_set_margin", "se_mlp_forward",
     "se_mlp_predict", "se_mlp_grad", "se_mlp_train", "se_mlp_save", "se_mlp_load", "se_normals_batch",
+    "se_get_batch_tuning", "se_set_batch_tuning", "se_tune_batch",
 ]
 MLP_FEATURES = 32
 MLP_PARAMS = 6337
@@ -54,7 +55,16 @@ class SeOptions(ctypes.Structure):
         ("batch_graph", ctypes.c_int32), ("debug_wait_limit", ctypes.c_int32),
         ("debug_inject", ctypes.c_int32), ("learned_cell_scan", ctypes.c_int32),
         ("cell_span", ctypes.c_int32), ("cell_max_points", ctypes.c_int32),
+        ("batch_lanes", ctypes.c_int32), ("batch_lane_min_points", ctypes.c_int32),
+        ("batch_blocks_per_sm", ctypes.c_int32), ("batch_warps_per_block", ctypes.c_int32),
     ]
+
+
+TUNING_FIELDS = ["leaf_bucket", "seed_halo", "lanes", "lane_min_points", "blocks_per_sm", "warps_per_block"]
+
+
+class SeBatchTuning(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int32) for n in TUNING_FIELDS]
 
 
 class SeInfo(ctypes.Structure):
@@ -137,6 +147,10 @@ def lib():
             "se_mlp_save": (i32, [P, ctypes.c_char_p]),
             "se_mlp_load": (i32, [P, ctypes.c_char_p]),
             "se_normals_batch": (i32, [P, P, P, P, P, i32, P, P, P, i32]),
+            "se_get_batch_tuning": (i32, [P, ctypes.POINTER(SeBatchTuning)]),
+            "se_set_batch_tuning": (i32, [P, ctypes.POINTER(SeBatchTuning)]),
+            "se_tune_batch": (i32, [P, P, P, P, P, i32, P, i32, i32, ctypes.POINTER(SeBatchTuning),
+                                    ctypes.POINTER(ctypes.c_float)]),
         }
         for name, (res, args) in sigs.items():
             fn = getattr(L, name)
@@ -169,7 +183,8 @@ class Context:
     def __init__(self, code_bits=63, root_compat=True, build_octree=True, viewpoint=(0.0, 0.0, 0.0),
                  eigengap_fp64=1e-4, leaf_bucket=96, device=0, stream=None, seed_halo=-1, learned=False,
                  learned_skip_seed=False, search_compat=False, batch_graph=True, debug_wait_limit=0,
-                 debug_inject=0, learned_cell_scan=False, cell_span=0, cell_max_points=0):
+                 debug_inject=0, learned_cell_scan=False, cell_span=0, cell_max_points=0, batch_lanes=0,
+                 batch_lane_min_points=0, batch_blocks_per_sm=0, batch_warps_per_block=0):
         L = lib()
         o = SeOptions()
         L.se_options_init(ctypes.byref(o))
@@ -192,6 +207,10 @@ class Context:
         o.learned_cell_scan = int(bool(learned_cell_scan))
         o.cell_span = int(cell_span)
         o.cell_max_points = int(cell_max_points)
+        o.batch_lanes = int(batch_lanes)
+        o.batch_lane_min_points = int(batch_lane_min_points)
+        o.batch_blocks_per_sm = int(batch_blocks_per_sm)
+        o.batch_warps_per_block = int(batch_warps_per_block)
         self.options = o
         h = ctypes.c_void_p()
         rc = L.se_create(ctypes.byref(h), ctypes.byref(o))
@@ -418,6 +437,36 @@ class Context:
         self._check(lib().se_normals_batch(self._h, px, _ptr(y)[0], _ptr(z)[0], _ptr(offsets)[0], n_clouds,
                                            _ptr(ks)[0], _ptr(out)[0], _ptr(u)[0], mem), "se_normals_batch")
         return out, offsets, u
+
+    def batch_tuning(self):
+        """The bucket, halo and batch scheduling se_normals_batch uses."""
+        t = SeBatchTuning()
+        self._check(lib().se_get_batch_tuning(self._h, ctypes.byref(t)), "se_get_batch_tuning")
+        return {n: getattr(t, n) for n in TUNING_FIELDS}
+
+    def set_batch_tuning(self, tuning):
+        t = SeBatchTuning(**{n: int(tuning[n]) for n in TUNING_FIELDS})
+        self._check(lib().se_set_batch_tuning(self._h, ctypes.byref(t)), "se_set_batch_tuning")
+
+    def tune_batch(self, clouds, ks, reps=3):
+        """se_tune_batch on this batch (the arguments of normals_batch): leaves
+        the fastest tuning set on the context; returns it with its time (ms)."""
+        if isinstance(ks, tuple):
+            ks, offsets = ks
+            x, y, z = clouds
+            offsets = np.ascontiguousarray(offsets, np.int64)
+        else:
+            sizes = [len(cl[0]) for cl in clouds]
+            offsets = np.zeros(len(clouds) + 1, np.int64)
+            offsets[1:] = np.cumsum(sizes)
+            x, y, z = (np.ascontiguousarray(np.concatenate([cl[i] for cl in clouds]), np.float32) for i in range(3))
+        ks = np.ascontiguousarray(ks, np.int32)
+        t = SeBatchTuning()
+        ms = ctypes.c_float()
+        px, mem = _ptr(x)
+        self._check(lib().se_tune_batch(self._h, px, _ptr(y)[0], _ptr(z)[0], _ptr(offsets)[0], ks.size, _ptr(ks)[0],
+                                        mem, int(reps), ctypes.byref(t), ctypes.byref(ms)), "se_tune_batch")
+        return {**{n: getattr(t, n) for n in TUNING_FIELDS}, "ms": float(ms.value)}
 
     def profile(self):
         p = SeProfile()

@@ -1,13 +1,16 @@
-"""Autotuner for the kNN kernel's tile parameters.
+"""Autotuner for the kNN kernel's tile parameters and the batch schedule.
 
 Two parameters shape the search kernel's work: `leaf_bucket` (subtrees of at
 most this many points are streamed as one tile) and `seed_halo` (Morton-window
 points offered on each side of a warp's 32 queries before the tree walk). The
-best pair depends on density and k, so it is measured, not guessed: every
-candidate is timed on the GPU (CUDA events around the build and the fused kNN
-+ normals kernel, median of `reps`) on the caller's own cloud or batch, and the
-winner is cached in a JSON file keyed by workload class (size decade, k, code
-bits), so that later runs reuse it without re-timing.
+batched path adds its schedule: stream lanes, the size above which a cloud is
+queried on its lane, and the persistent launches' resident blocks per SM and
+warps per block. The best values depend on density, k and the batch's size
+mix, so they are measured, not guessed, on the caller's own cloud or batch
+(single clouds here with CUDA events around the build and the fused kNN +
+normals kernel; batches in the library, se_tune_batch), and the winner is
+cached in a JSON file keyed by workload class (size decade, k, code bits,
+cloud count), so that later runs reuse it without re-timing.
 """
 from __future__ import annotations
 
@@ -72,29 +75,39 @@ def tune_cloud(x, y, z, k, code_bits=63, device=0, cache_path=DEFAULT_CACHE, rep
     return entry
 
 
-def tune_batch(clouds, ks, code_bits=63, device=0, cache_path=DEFAULT_CACHE, reps=2, force=False):
-    """Best (leaf_bucket, seed_halo) for a batch of clouds (se_normals_batch)."""
-    sizes = [len(c[0]) for c in clouds]
-    key = "batch_" + workload_key(int(np.sum(sizes)), int(np.max(ks)), code_bits) + f"_c{len(clouds)}"
+def batch_key(clouds, ks, code_bits=63) -> str:
+    """Class of a batch given as normals_batch takes it: a list of (x, y, z)
+    clouds, or concatenated (x, y, z) with ks=(ks, offsets)."""
+    if isinstance(ks, tuple):
+        ks, offsets = ks
+        total, n = int(offsets[-1]), len(ks)
+    else:
+        total, n = int(np.sum([len(c[0]) for c in clouds])), len(clouds)
+    return "batch_" + workload_key(total, int(np.max(ks)), code_bits) + f"_c{n}"
+
+
+def tune_batch(clouds, ks, code_bits=63, device=0, cache_path=DEFAULT_CACHE, reps=2, force=False, ctx=None):
+    """Best se_normals_batch tuning for this batch's class: bucket size, seed
+    halo, stream lanes, the per-lane query cut-off, and the persistent
+    launches' resident blocks and block shape. The search runs in the library
+    (se_tune_batch: CUDA events around whole batched calls, one parameter at
+    a time over two rounds); the winner is cached per class and, when `ctx`
+    is given, left set on it."""
+    key = batch_key(clouds, ks, code_bits)
     table = _load(cache_path) if cache_path else {}
     if key in table and not force:
-        return table[key]
-    results = []
-    for bucket, halo in CANDIDATES:
-        with Context(code_bits=code_bits, device=device, leaf_bucket=bucket, seed_halo=halo) as ctx:
-            import time
-
-            times = []
-            for _ in range(reps + 1):
-                ctx.synchronize()
-                t0 = time.perf_counter()
-                ctx.normals_batch(clouds, ks)
-                times.append((time.perf_counter() - t0) * 1e3)
-            results.append((statistics.median(times[1:]), bucket, halo))
-    ms, bucket, halo = min(results)
-    entry = {"leaf_bucket": bucket, "seed_halo": halo, "ms": ms,
-             "timings": [{"leaf_bucket": b, "seed_halo": h, "ms": t} for t, b, h in results]}
-    if cache_path:
-        table[key] = entry
-        _save(cache_path, table)
+        entry = table[key]
+    else:
+        own = ctx is None
+        c = Context(code_bits=code_bits, device=device) if own else ctx
+        try:
+            entry = c.tune_batch(clouds, ks, reps=reps)
+        finally:
+            if own:
+                c.close()
+        if cache_path:
+            table[key] = entry
+            _save(cache_path, table)
+    if ctx is not None:
+        ctx.set_batch_tuning(entry)
     return entry

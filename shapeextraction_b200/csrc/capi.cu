@@ -348,6 +348,10 @@ int se_create(se_ctx** out, const se_options* opt) {
     if (o.learned_cell_scan != 0 && o.learned_cell_scan != 1) return SE_ERR_INVALID_ARG;
     if (o.cell_span != 0 && (o.cell_span < 2 || o.cell_span > 4)) return SE_ERR_INVALID_ARG;
     if (o.cell_max_points < 0) return SE_ERR_INVALID_ARG;
+    if (o.batch_lanes < 0 || o.batch_lanes > 16 || o.batch_lane_min_points < 0 || o.batch_blocks_per_sm < 0 ||
+        o.batch_blocks_per_sm > 32 ||
+        (o.batch_warps_per_block != 0 && o.batch_warps_per_block != 2 && o.batch_warps_per_block != 4))
+        return SE_ERR_INVALID_ARG;
     if (o.debug_inject & ~(SE_DEBUG_STALL_SORT_TILE | SE_DEBUG_SEARCH_LIMIT | SE_DEBUG_ALLOC_FAIL))
         return SE_ERR_INVALID_ARG;
     se_ctx* c = new se_ctx();

@@ -18,6 +18,11 @@ extern "C" {
 
 namespace {
 
+int batch_lanes(const se_ctx* c) { return c->opt.batch_lanes > 0 ? c->opt.batch_lanes : 8; }
+int64_t batch_lane_min(const se_ctx* c) {
+    return c->opt.batch_lane_min_points > 0 ? (int64_t)c->opt.batch_lane_min_points : 65536;
+}
+
 int lane_capacity(se_ctx* c, BatchLane& l, int64_t n) {
     if (!l.stream) {
         SE_CUDA(c, cudaStreamCreateWithFlags(&l.stream, cudaStreamNonBlocking), "lane stream");
@@ -166,6 +171,8 @@ int enqueue_batch(se_ctx* c, const BatchPlan& plan, const BatchCloud* d_desc, co
         q.code_bits = c->opt.code_bits;
         q.bucket = c->opt.leaf_bucket;
         q.seed_halo = seed_halo_for(c, q.k);
+        q.batch_blocks_per_sm = c->opt.batch_blocks_per_sm;
+        q.batch_warps_per_block = c->opt.batch_warps_per_block;
         const int first = plan.group_first[gi], count = plan.group_first[gi + 1] - first;
         SE_CUDA(c, enqueue_query_batch(d_desc + first, count, plan.group_items[gi], c->batch_counter + gi, q, g,
                                        c->num_sms),
@@ -258,10 +265,10 @@ int se_normals_batch(se_ctx* c, const float* x, const float* y, const float* z, 
     // lanes still build later groups. Lanes take the large clouds first, then
     // the small ones group by group; largest cloud first, each to the lane
     // with the least queued work.
-    constexpr int64_t kLaneQueryMin = 65536;
+    const int64_t kLaneQueryMin = batch_lane_min(c);
     BatchPlan plan;
     plan.lane_query.assign(n_clouds, 0);
-    plan.n_lanes = std::min(n_clouds, 8);
+    plan.n_lanes = std::min(n_clouds, batch_lanes(c));
     if ((int)c->lanes.size() < plan.n_lanes) c->lanes.resize(plan.n_lanes);
     std::vector<int> order(n_clouds);
     std::iota(order.begin(), order.end(), 0);
@@ -345,6 +352,13 @@ int se_normals_batch(se_ctx* c, const float* x, const float* y, const float* z, 
     key.push_back((int64_t)(uintptr_t)z);
     key.push_back((int64_t)(uintptr_t)out_normals);
     key.push_back((int64_t)c->batch_epoch);
+    // the tuning changes the launches
+    key.push_back(c->opt.leaf_bucket);
+    key.push_back(c->opt.seed_halo);
+    key.push_back(batch_lanes(c));
+    key.push_back(kLaneQueryMin);
+    key.push_back(c->opt.batch_blocks_per_sm);
+    key.push_back(c->opt.batch_warps_per_block);
     key.insert(key.end(), offsets, offsets + n_clouds + 1);
     key.insert(key.end(), ks, ks + n_clouds);
     const bool graphable = c->opt.batch_graph && total > 0 &&
@@ -433,6 +447,125 @@ int se_normals_batch(se_ctx* c, const float* x, const float* y, const float* z, 
         err |= c->h_batch_err[i];
     }
     return check_err_bits(c, err);
+}
+
+int se_get_batch_tuning(const se_ctx* c, se_batch_tuning* t) {
+    if (!c || !t) return SE_ERR_INVALID_ARG;
+    t->leaf_bucket = c->opt.leaf_bucket;
+    t->seed_halo = c->opt.seed_halo;
+    t->lanes = batch_lanes(c);
+    t->lane_min_points = (int32_t)batch_lane_min(c);
+    t->blocks_per_sm = c->opt.batch_blocks_per_sm;
+    t->warps_per_block = c->opt.batch_warps_per_block;
+    return SE_OK;
+}
+
+int se_set_batch_tuning(se_ctx* c, const se_batch_tuning* t) {
+    if (!c || !t) return SE_ERR_INVALID_ARG;
+    if (t->leaf_bucket < 1 || t->leaf_bucket > 128 || t->seed_halo < -1 || t->seed_halo > 48 || t->lanes < 0 ||
+        t->lanes > 16 || t->lane_min_points < 0 || t->blocks_per_sm < 0 || t->blocks_per_sm > 32 ||
+        (t->warps_per_block != 0 && t->warps_per_block != 2 && t->warps_per_block != 4))
+        return fail(c, SE_ERR_INVALID_ARG, "batch tuning out of range");
+    c->opt.leaf_bucket = t->leaf_bucket;
+    c->opt.seed_halo = t->seed_halo;
+    c->opt.batch_lanes = t->lanes;
+    c->opt.batch_lane_min_points = t->lane_min_points;
+    c->opt.batch_blocks_per_sm = t->blocks_per_sm;
+    c->opt.batch_warps_per_block = t->warps_per_block;
+    return SE_OK;
+}
+
+int se_tune_batch(se_ctx* c, const float* x, const float* y, const float* z, const int64_t* offsets, int n_clouds,
+                  const int32_t* ks, int mem, int reps, se_batch_tuning* best, float* best_ms) {
+    NvtxRange nvtx("shapex.se_tune_batch");
+    if (int rc = prologue(c)) return rc;
+    if (int rc = check_mem(c, mem)) return rc;
+    if (n_clouds < 1 || !offsets || !ks) return fail(c, SE_ERR_INVALID_ARG, "bad batch description");
+    if (reps < 1) reps = 1;
+    const int64_t total = offsets[n_clouds];
+    if (total < 0 || total > ((int64_t)1 << 30)) return fail(c, SE_ERR_INVALID_ARG, "bad batch size");
+    // outputs like the caller's: device memory, or pinned host memory
+    float* out = nullptr;
+    const bool host = mem == SE_MEM_HOST;
+    const size_t out_bytes = sizeof(float) * 3 * (size_t)(total > 0 ? total : 1);
+    cudaError_t e = host ? cudaMallocHost(&out, out_bytes) : cudaMalloc(&out, out_bytes);
+    if (e != cudaSuccess) return cuda_fail(c, e, "alloc tuner output");
+    std::vector<int64_t> u(n_clouds);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    se_batch_tuning orig{}, cur{};
+    se_get_batch_tuning(c, &orig);
+    cur = orig;
+    int rc = SE_OK;
+    // median over reps of one configuration (a first untimed call records its graph)
+    auto measure = [&](const se_batch_tuning& t, float& ms) -> int {
+        if (int r = se_set_batch_tuning(c, &t)) return r;
+        if (int r = se_normals_batch(c, x, y, z, offsets, n_clouds, ks, out, u.data(), mem)) return r;
+        std::vector<float> ts;
+        for (int i = 0; i < reps; ++i) {
+            cudaEventRecord(e0, c->stream);
+            if (int r = se_normals_batch(c, x, y, z, offsets, n_clouds, ks, out, u.data(), mem)) return r;
+            cudaEventRecord(e1, c->stream);
+            const cudaError_t ce = cudaEventSynchronize(e1);
+            if (ce != cudaSuccess) return cuda_fail(c, ce, "time batch");
+            float t_ms = 0.0f;
+            cudaEventElapsedTime(&t_ms, e0, e1);
+            ts.push_back(t_ms);
+        }
+        std::sort(ts.begin(), ts.end());
+        ms = ts[ts.size() / 2];
+        return SE_OK;
+    };
+    float cur_ms = 0.0f;
+    rc = measure(cur, cur_ms);
+    // coordinate descent, two rounds: each parameter over its values, the others fixed
+    static const int kBucket[] = {48, 64, 96, 128};
+    static const int kHalo[] = {-1, 8, 16, 32};
+    static const int kLanes[] = {4, 8, 16};
+    static const int kLaneMin[] = {32768, 65536, 131072, 262144};
+    static const int kBlocks[] = {0, 2, 3, 4};
+    static const int kWarps[] = {2, 4};
+    for (int round = 0; round < 2 && rc == SE_OK; ++round) {
+        for (int dim = 0; dim < 6 && rc == SE_OK; ++dim) {
+            const int* vals;
+            int nv;
+            int32_t se_batch_tuning::*field;
+            switch (dim) {
+                case 0: vals = kBucket; nv = 4; field = &se_batch_tuning::leaf_bucket; break;
+                case 1: vals = kHalo; nv = 4; field = &se_batch_tuning::seed_halo; break;
+                case 2: vals = kLanes; nv = 3; field = &se_batch_tuning::lanes; break;
+                case 3: vals = kLaneMin; nv = 4; field = &se_batch_tuning::lane_min_points; break;
+                case 4: vals = kBlocks; nv = 4; field = &se_batch_tuning::blocks_per_sm; break;
+                default: vals = kWarps; nv = 2; field = &se_batch_tuning::warps_per_block; break;
+            }
+            for (int vi = 0; vi < nv && rc == SE_OK; ++vi) {
+                if (cur.*field == vals[vi]) continue;
+                se_batch_tuning t = cur;
+                t.*field = vals[vi];
+                float ms = 0.0f;
+                rc = measure(t, ms);
+                if (rc == SE_OK && ms < cur_ms) {
+                    cur = t;
+                    cur_ms = ms;
+                }
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (host) cudaFreeHost(out);
+    else cudaFree(out);
+    if (rc != SE_OK) {
+        const std::string msg = c->last_error;
+        se_set_batch_tuning(c, &orig);
+        c->last_error = msg;
+        return rc;
+    }
+    se_set_batch_tuning(c, &cur);
+    if (best) *best = cur;
+    if (best_ms) *best_ms = cur_ms;
+    return SE_OK;
 }
 
 }  // extern "C"

@@ -95,22 +95,44 @@ struct TopK {
     // odd-even transposition network (K passes of independent
     // compare-exchanges) and set the bound.
     __device__ __forceinline__ void sort_filled() {
-        // K passes as K/2 rolled (even, odd) pairs: the same exchanges as a
-        // fully unrolled network in K instead of K*K/2 instructions' worth of
-        // code, which keeps large-k kernels inside the instruction cache
+        if constexpr (K == 4 || K == 8 || K == 16) {
+            // power-of-two lists: a bitonic network, fully unrolled (80
+            // compare-exchanges at K = 16 against 120 for the transposition
+            // network below, in about as much code)
+#pragma unroll
+            for (int k = 2; k <= K; k <<= 1)
+#pragma unroll
+                for (int j = k >> 1; j > 0; j >>= 1)
+#pragma unroll
+                    for (int i = 0; i < K; ++i) {
+                        const int l = i ^ j;
+                        if (l > i) {
+                            const unsigned long long a = key[i], b = key[l];
+                            const bool up = (i & k) == 0;
+                            const bool sw = up ? (b < a) : (a < b);
+                            key[i] = sw ? b : a;
+                            key[l] = sw ? a : b;
+                        }
+                    }
+        } else {
+            // K passes as K/2 rolled (even, odd) pairs: the same exchanges as
+            // a fully unrolled network in K instead of K*K/2 instructions'
+            // worth of code, which keeps large-k kernels inside the
+            // instruction cache
 #pragma unroll 1
-        for (int pass = 0; pass < K; pass += 2) {
+            for (int pass = 0; pass < K; pass += 2) {
 #pragma unroll
-            for (int j = 0; j + 1 < K; j += 2) {
-                const unsigned long long a = key[j], b = key[j + 1];
-                key[j] = a < b ? a : b;
-                key[j + 1] = a < b ? b : a;
-            }
+                for (int j = 0; j + 1 < K; j += 2) {
+                    const unsigned long long a = key[j], b = key[j + 1];
+                    key[j] = a < b ? a : b;
+                    key[j + 1] = a < b ? b : a;
+                }
 #pragma unroll
-            for (int j = 1; j + 1 < K; j += 2) {
-                const unsigned long long a = key[j], b = key[j + 1];
-                key[j] = a < b ? a : b;
-                key[j + 1] = a < b ? b : a;
+                for (int j = 1; j + 1 < K; j += 2) {
+                    const unsigned long long a = key[j], b = key[j + 1];
+                    key[j] = a < b ? a : b;
+                    key[j + 1] = a < b ? b : a;
+                }
             }
         }
         if (EXACT) {
@@ -305,6 +327,30 @@ __device__ __forceinline__ void axis_bounds(uint32_t X0, uint32_t X1, float inv_
     hi = __fmaf_rn((float)X1 * inv_m, range, mn) + pad;
 }
 
+// Integer code-coordinate box [lo, hi] (per axis, clamped to [0, M]) that
+// holds every tree point within squared distance r2 of the tree point whose
+// code is `code`: |x_p - x_q| <= R for every point p with dist2 <= r2
+// (dist2's rounding costs far less than the 1e-6 added to R), and in code
+// units the decode adds at most 1/4 + 2^-23 * M * max|coordinate| / range on
+// each side. r2 must be finite and >= 0; a degenerate range gives the whole
+// cube.
+__device__ __forceinline__ void ball_box(uint64_t code, float r2, uint32_t M, float mn, float range, uint32_t (&lo)[3],
+                                         uint32_t (&hi)[3]) {
+    const float fbs = (float)M;
+    const float R = __fmul_ru(__fsqrt_ru(r2), 1.000001f);
+    const float ru = __fmul_ru(R, __fdiv_ru(fbs, range));
+    const float big = fmaxf(fabsf(mn), fabsf(mn + range));
+    const float slack = __fadd_ru(__fmul_ru(__fmul_ru(1.1920929e-7f, fbs), __fdiv_ru(big, range)), 0.25f);
+    const float ext = __fadd_ru(ru, slack) + 1.0f;
+    const int64_t e = ext < 4.0e9f ? (int64_t)ceilf(ext) : ((int64_t)1 << 40);  // NaN: whole cube
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+        const int64_t X = (int64_t)gather3(code >> ax);
+        lo[ax] = (uint32_t)max64(0, X - e);
+        hi[ax] = (uint32_t)min64((int64_t)M, X + e);
+    }
+}
+
 constexpr int kCellBits = 1024;   // cells of a warp's union grid: one bit each, in stack[0, 32)
 constexpr int kCellRanges = 64;   // nonempty cells a warp scans: listed in pts[32, 96), order keys after
 
@@ -340,24 +386,10 @@ __device__ __forceinline__ bool cell_scan(TopK<K, EXACT>& tk, int& bc, WS& W, in
     uint32_t lo[3] = {0u, 0u, 0u}, hi[3] = {0u, 0u, 0u};
     int s = 0;
     if (ok) {
-        // |x_p - x_q| <= R for every point within the cap (dist2's rounding
-        // costs far less than the 1e-6 added); in code units the decode adds
-        // at most 1/4 + 2^-23 * M * max|coordinate| / range on each side.
-        const float R = __fmul_ru(__fsqrt_ru(cap), 1.000001f);
-        const float ru = __fmul_ru(R, __fdiv_ru(fbs, range));
-        const float big = fmaxf(fabsf(mn), fabsf(mn + range));
-        const float slack = __fadd_ru(__fmul_ru(__fmul_ru(1.1920929e-7f, fbs), __fdiv_ru(big, range)), 0.25f);
-        const float ext = __fadd_ru(ru, slack) + 1.0f;
-        const int64_t e = ext < 4.0e9f ? (int64_t)ceilf(ext) : ((int64_t)1 << 40);  // NaN range: whole cube
-        const uint64_t code = __ldg(codes + qi);
+        ball_box(__ldg(codes + qi), cap, M, mn, range, lo, hi);
         uint32_t dmax = 0;
 #pragma unroll
-        for (int ax = 0; ax < 3; ++ax) {
-            const int64_t X = (int64_t)gather3(code >> ax);
-            lo[ax] = (uint32_t)max64(0, X - e);
-            hi[ax] = (uint32_t)min64((int64_t)M, X + e);
-            dmax = max(dmax, hi[ax] - lo[ax]);
-        }
+        for (int ax = 0; ax < 3; ++ax) dmax = max(dmax, hi[ax] - lo[ax]);
         // the finest level at which the box spans at most cell_span cells per
         // axis: (hi >> s) - (lo >> s) <= (dmax >> s) + 1 <= cell_span - 1
         while ((int)(dmax >> s) > a.cell_span - 2) ++s;
@@ -882,8 +914,18 @@ __global__ void __launch_bounds__(KnnCfg<K>::threads, KnnCfg<K>::min_blocks)
 // cloud by cloud in the order of `clouds` (largest first), so the large clouds
 // start first and the small ones fill the tail. Each cloud's size is read on
 // the device from its own build state.
-template <int K, bool EXACT>
-__global__ void __launch_bounds__(KnnCfg<K>::threads, KnnCfg<K>::min_blocks)
+// Block shape of the persistent launch: W warps per block, with the
+// resident-block target scaled so that ptxas gets the same register budget
+// per thread as the per-k default shape (KnnCfg).
+template <int K, int W>
+struct BatchCfg {
+    static constexpr int threads = 32 * W;
+    static constexpr int min_blocks =
+        (KnnCfg<K>::min_blocks * KnnCfg<K>::warps) / W > 0 ? (KnnCfg<K>::min_blocks * KnnCfg<K>::warps) / W : 1;
+};
+
+template <int K, bool EXACT, int NW>
+__global__ void __launch_bounds__(BatchCfg<K, NW>::threads, BatchCfg<K, NW>::min_blocks)
     k_knn_batch(const BatchCloud* __restrict__ clouds, int n_clouds,
                                                            int64_t n_items, unsigned long long* counter, QArgs a) {
     extern __shared__ __align__(16) unsigned char knn_smem[];
@@ -906,8 +948,8 @@ __global__ void __launch_bounds__(KnnCfg<K>::threads, KnnCfg<K>::min_blocks)
         ca.out_normals = d.out_normals;
         ca.start = 0;
         ca.device_count = 1;
-        knn_warp<K, EXACT, false, true, false>(d.pts, d.snodes, nullptr, ca, d.st, ((int64_t)item - d.item0) * 32, W,
-                                               lane);
+        knn_warp<K, EXACT, false, true, false>(d.pts, d.snodes, nullptr, ca, d.st, ((int64_t)item - d.item0) * 32,
+                                               W, lane);
         __syncwarp();
     }
 }
@@ -936,22 +978,37 @@ cudaError_t launch_k(const BuildBufs& b, const QArgs& a, bool ext, bool normals,
     return launch_one<K, EXACT, false, false>(b, a, blocks, s);
 }
 
-template <int K, bool EXACT>
-cudaError_t launch_batch(const BatchCloud* clouds, int n_clouds, int64_t n_items, unsigned long long* counter,
-                         const QArgs& a, cudaStream_t s, int num_sms) {
-    constexpr int smem = (int)sizeof(WarpSmem<KnnCfg<K>::buf>) * KnnCfg<K>::warps;
-    cudaError_t e = cudaFuncSetAttribute(k_knn_batch<K, EXACT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+template <int K, bool EXACT, int NW>
+cudaError_t launch_batch_w(const BatchCloud* clouds, int n_clouds, int64_t n_items, unsigned long long* counter,
+                           const QArgs& a, cudaStream_t s, int num_sms, int blocks_per_sm) {
+    constexpr int threads = BatchCfg<K, NW>::threads;
+    constexpr int smem = (int)sizeof(WarpSmem<KnnCfg<K>::buf>) * NW;
+    cudaError_t e =
+        cudaFuncSetAttribute(k_knn_batch<K, EXACT, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_knn_batch<K, EXACT>, KnnCfg<K>::threads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_knn_batch<K, EXACT, NW>, threads, smem);
     if (e != cudaSuccess) return e;
-    const int64_t want = (n_items + KnnCfg<K>::warps - 1) / KnnCfg<K>::warps;
-    const int64_t resident = (int64_t)(per_sm > 0 ? per_sm : 1) * num_sms;
+    if (per_sm < 1) per_sm = 1;
+    if (blocks_per_sm > 0 && blocks_per_sm < per_sm) per_sm = blocks_per_sm;
+    const int64_t want = (n_items + NW - 1) / NW;
+    const int64_t resident = (int64_t)per_sm * num_sms;
     const unsigned blocks = (unsigned)(want < resident ? want : resident);
     e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s);
     if (e != cudaSuccess) return e;
-    k_knn_batch<K, EXACT><<<blocks, KnnCfg<K>::threads, smem, s>>>(clouds, n_clouds, n_items, counter, a);
+    k_knn_batch<K, EXACT, NW><<<blocks, threads, smem, s>>>(clouds, n_clouds, n_items, counter, a);
     return cudaGetLastError();
+}
+
+// The per-k default block shape, or the other one of 2 and 4 warps.
+template <int K, bool EXACT>
+cudaError_t launch_batch(const BatchCloud* clouds, int n_clouds, int64_t n_items, unsigned long long* counter,
+                         const QArgs& a, cudaStream_t s, int num_sms, int blocks_per_sm, int warps) {
+    constexpr int def = KnnCfg<K>::warps;
+    constexpr int alt = def == 4 ? 2 : 4;
+    if (warps == alt) return launch_batch_w<K, EXACT, alt>(clouds, n_clouds, n_items, counter, a, s, num_sms,
+                                                           blocks_per_sm);
+    return launch_batch_w<K, EXACT, def>(clouds, n_clouds, n_items, counter, a, s, num_sms, blocks_per_sm);
 }
 
 // lut[j] = lower bound of j << sh in the u sorted unique codes, for j in
@@ -1007,19 +1064,20 @@ cudaError_t enqueue_query_batch(const BatchCloud* clouds, int n_clouds, int64_t 
     a.bucket = q.bucket;
     a.seed_halo = q.seed_halo < 0 ? 0 : (q.seed_halo > kMaxHalo ? kMaxHalo : q.seed_halo);
     a.device_count = 1;
+    const int bps = q.batch_blocks_per_sm, wpb = q.batch_warps_per_block;
     switch (q.k) {
-        case 8: return launch_batch<8, true>(clouds, n_clouds, n_items, counter, a, s, num_sms);
-        case 10: return launch_batch<10, true>(clouds, n_clouds, n_items, counter, a, s, num_sms);
-        case 16: return launch_batch<16, true>(clouds, n_clouds, n_items, counter, a, s, num_sms);
-        case 32: return launch_batch<32, true>(clouds, n_clouds, n_items, counter, a, s, num_sms);
+        case 8: return launch_batch<8, true>(clouds, n_clouds, n_items, counter, a, s, num_sms, bps, wpb);
+        case 10: return launch_batch<10, true>(clouds, n_clouds, n_items, counter, a, s, num_sms, bps, wpb);
+        case 16: return launch_batch<16, true>(clouds, n_clouds, n_items, counter, a, s, num_sms, bps, wpb);
+        case 32: return launch_batch<32, true>(clouds, n_clouds, n_items, counter, a, s, num_sms, bps, wpb);
         default: break;
     }
-    if (q.k <= 4) return launch_batch<4, false>(clouds, n_clouds, n_items, counter, a, s, num_sms);
-    if (q.k <= 8) return launch_batch<8, false>(clouds, n_clouds, n_items, counter, a, s, num_sms);
-    if (q.k <= 12) return launch_batch<12, false>(clouds, n_clouds, n_items, counter, a, s, num_sms);
-    if (q.k <= 16) return launch_batch<16, false>(clouds, n_clouds, n_items, counter, a, s, num_sms);
-    if (q.k <= 24) return launch_batch<24, false>(clouds, n_clouds, n_items, counter, a, s, num_sms);
-    return launch_batch<32, false>(clouds, n_clouds, n_items, counter, a, s, num_sms);
+    if (q.k <= 4) return launch_batch<4, false>(clouds, n_clouds, n_items, counter, a, s, num_sms, bps, wpb);
+    if (q.k <= 8) return launch_batch<8, false>(clouds, n_clouds, n_items, counter, a, s, num_sms, bps, wpb);
+    if (q.k <= 12) return launch_batch<12, false>(clouds, n_clouds, n_items, counter, a, s, num_sms, bps, wpb);
+    if (q.k <= 16) return launch_batch<16, false>(clouds, n_clouds, n_items, counter, a, s, num_sms, bps, wpb);
+    if (q.k <= 24) return launch_batch<24, false>(clouds, n_clouds, n_items, counter, a, s, num_sms, bps, wpb);
+    return launch_batch<32, false>(clouds, n_clouds, n_items, counter, a, s, num_sms, bps, wpb);
 }
 
 cudaError_t enqueue_query(const BuildBufs& b, const QueryParams& q, cudaStream_t s, int /*num_sms*/) {

@@ -1,10 +1,11 @@
 // Learned search-radius proposal: per-point occupancy features and a 3-layer
 // MLP (32 -> 64 -> 64 -> 1, BF16 weights and activations, FP32 accumulation)
 // that predicts log2(r_k^2 / range^2), the squared distance to a point's k-th
-// neighbour in units of the cloud's extent. Training (forward, backward,
-// weight-gradient reductions, Adam) and inference are kernels of this file;
-// inference runs the two hidden layers on the tensor cores (mma.sync
-// m16n8k16, BF16 in, FP32 accumulate), fused with the feature computation.
+// neighbour in units of the cloud's extent. Training (a fused forward,
+// backward and weight-gradient step, then Adam) and inference are kernels of
+// this file; both run their contractions on the tensor cores (mma.sync
+// m16n8k16, BF16 in, FP32 accumulate); inference is fused with the feature
+// computation.
 // The exact kNN search uses the prediction only as a starting bound and falls
 // back to the plain search for any query whose k-th neighbour lies beyond it.
 
@@ -90,9 +91,10 @@ __global__ void __launch_bounds__(256) k_features(const float4* __restrict__ pts
 }
 
 // ---------------------------------------------------------------------------
-// Training path (CUDA cores, FP32 accumulation over BF16-rounded weights,
-// inputs and activations: the same numbers the tensor-core inference uses).
-// Parameter layout (FP32 master copy): see MlpLayout in pipeline.cuh.
+// Forward on the CUDA cores (FP32 accumulation in a fixed fmaf order over
+// BF16-rounded weights, inputs and activations), for se_mlp_forward: the
+// calibration of the margin and the oracle check use it. Parameter layout
+// (FP32 master copy): see MlpLayout in pipeline.cuh.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(128) k_mlp_forward(const float* __restrict__ params, const float* __restrict__ X,
                                                      int64_t n, float* __restrict__ yhat, float* __restrict__ h1_out,
@@ -132,77 +134,6 @@ __global__ void __launch_bounds__(128) k_mlp_forward(const float* __restrict__ p
     if (h1_out)
         for (int i = 0; i < kMlpH; ++i) h1_out[r * kMlpH + i] = h1[i];
     yhat[r] = y;
-}
-
-// Per-sample output and hidden-layer gradients of the mean squared error
-// loss = mean((yhat - y)^2); accumulates the bias gradients and the loss.
-__global__ void __launch_bounds__(128) k_mlp_backward_rows(const float* __restrict__ params,
-                                                           const float* __restrict__ yhat,
-                                                           const float* __restrict__ y, const float* __restrict__ h1,
-                                                           const float* __restrict__ h2, int64_t n,
-                                                           float* __restrict__ dy_out, float* __restrict__ dh1_out,
-                                                           float* __restrict__ dh2_out, float* __restrict__ grads,
-                                                           float* __restrict__ loss) {
-    __shared__ float sW2[kMlpH * kMlpH], sw3[kMlpH], sdb1[kMlpH], sdb2[kMlpH];
-    __shared__ float sdb3, sloss;
-    for (int i = threadIdx.x; i < kMlpH * kMlpH; i += blockDim.x) sW2[i] = bf16r(params[MlpLayout::W2 + i]);
-    for (int i = threadIdx.x; i < kMlpH; i += blockDim.x) {
-        sw3[i] = bf16r(params[MlpLayout::W3 + i]);
-        sdb1[i] = 0.0f;
-        sdb2[i] = 0.0f;
-    }
-    if (threadIdx.x == 0) { sdb3 = 0.0f; sloss = 0.0f; }
-    __syncthreads();
-    const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (r < n) {
-        const float e = yhat[r] - y[r];
-        const float dy = 2.0f * e / (float)n;
-        dy_out[r] = dy;
-        atomicAdd(&sloss, e * e / (float)n);
-        atomicAdd(&sdb3, dy);
-        float dh2[kMlpH];
-#pragma unroll 8
-        for (int i = 0; i < kMlpH; ++i) {
-            dh2[i] = h2[r * kMlpH + i] > 0.0f ? dy * sw3[i] : 0.0f;
-            dh2_out[r * kMlpH + i] = dh2[i];
-            atomicAdd(&sdb2[i], dh2[i]);
-        }
-        for (int j = 0; j < kMlpH; ++j) {
-            float a = 0.0f;
-            if (h1[r * kMlpH + j] > 0.0f) {
-#pragma unroll 8
-                for (int i = 0; i < kMlpH; ++i) a = fmaf(sW2[j * kMlpH + i], dh2[i], a);
-            }
-            dh1_out[r * kMlpH + j] = a;
-            atomicAdd(&sdb1[j], a);
-        }
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i < kMlpH; i += blockDim.x) {
-        atomicAdd(&grads[MlpLayout::B1 + i], sdb1[i]);
-        atomicAdd(&grads[MlpLayout::B2 + i], sdb2[i]);
-    }
-    if (threadIdx.x == 0) {
-        atomicAdd(&grads[MlpLayout::B3], sdb3);
-        atomicAdd(loss, sloss);
-    }
-}
-
-// Weight gradient G[a][b] += sum_r A[r][a] * D[r][b] (A: n x na, D: n x nb),
-// one thread per output entry, rows split over blocks along y.
-__global__ void __launch_bounds__(256) k_mlp_outer(const float* __restrict__ A, int na, const float* __restrict__ D,
-                                                   int nb, int64_t n, bool bf16_a, float* __restrict__ G) {
-    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= na * nb) return;
-    const int ia = idx / nb, ib = idx % nb;
-    const int64_t rows_per = (n + gridDim.y - 1) / gridDim.y;
-    const int64_t r0 = blockIdx.y * rows_per, r1 = min64(n, r0 + rows_per);
-    float acc = 0.0f;
-    for (int64_t r = r0; r < r1; ++r) {
-        const float a = A[r * na + ia];
-        acc = fmaf(bf16_a ? bf16r(a) : a, D[r * nb + ib], acc);
-    }
-    atomicAdd(&G[idx], acc);
 }
 
 // Adam (Kingma & Ba, 2015) on the FP32 master parameters.
@@ -367,6 +298,221 @@ __global__ void __launch_bounds__(128) k_predict_radius(const float* __restrict_
     }
 }
 
+// ---------------------------------------------------------------------------
+// Training step on the tensor cores: forward, backward and weight gradients of
+// the mean squared error for one batch in one kernel. A warp takes 32 rows at
+// a time: both hidden layers, dh1 = (h1 > 0) * (dh2 W2^T) and the weight
+// gradients dW1 = X^T dh1 and dW2 = h1^T dh2 (K = the 32 rows) are
+// mma.sync.m16n8k16 products over BF16 tiles in shared memory (row-major tiles
+// for the layers, transposed ones for the gradients) with FP32 accumulation;
+// dh1 and dh2 enter the weight gradients rounded to BF16, the bias gradients
+// unrounded. Each warp's gradient tiles are added to the FP32 gradient
+// vector with reductions; the bias, w3 and loss terms are reduced across the
+// warp first.
+// ---------------------------------------------------------------------------
+struct MlpTrainSmem {
+    __nv_bfloat16 w1t[kMlpH][kMlpF + 8];  // forward layer 1: [out][in]
+    __nv_bfloat16 w2t[kMlpH][kMlpH + 8];  // forward layer 2: [out][in]
+    __nv_bfloat16 w2n[kMlpH][kMlpH + 8];  // backward: W2 as stored, [in][out]
+    float b1[kMlpH], b2[kMlpH], w3[kMlpH];
+    struct Warp {
+        __nv_bfloat16 x[32][kMlpF + 8];   // [row][feature]
+        __nv_bfloat16 xt[kMlpF][32 + 8];  // [feature][row]
+        __nv_bfloat16 h1[32][kMlpH + 8];  // [row][unit]
+        __nv_bfloat16 h1t[kMlpH][32 + 8]; // [unit][row]
+        __nv_bfloat16 d2[32][kMlpH + 8];  // dh2 [row][unit]
+        __nv_bfloat16 d2t[kMlpH][32 + 8];
+        __nv_bfloat16 d1t[kMlpH][32 + 8]; // dh1 [unit][row]
+        float sums[3][kMlpH];             // this warp's b1, b2 and w3 gradient sums
+    } w[4];
+};
+
+// Sum v over the 8 row groups of the lanes (lanes with the same t), and add
+// the total of each column nb * 8 + 2t + b to dst[col] on the lanes of group 0.
+__device__ __forceinline__ void add_columns(float (&v)[16], float* __restrict__ dst, int lane) {
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+#pragma unroll
+        for (int o = 4; o < 32; o <<= 1) v[i] += __shfl_xor_sync(FULL, v[i], o);
+    if ((lane >> 2) == 0) {
+        const int t = lane & 3;
+#pragma unroll
+        for (int nb = 0; nb < 8; ++nb)
+#pragma unroll
+            for (int b = 0; b < 2; ++b) dst[nb * 8 + 2 * t + b] += v[nb * 2 + b];
+    }
+}
+
+// grads[base + row * kMlpH + col] += acc (the 32 x 64 product of mma_layer),
+// rows offset by row0.
+__device__ __forceinline__ void add_tile(float* __restrict__ grads, int base, int row0, const float (&acc)[2][8][4],
+                                         int lane) {
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int mb = 0; mb < 2; ++mb)
+#pragma unroll
+        for (int nb = 0; nb < 8; ++nb)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int row = row0 + mb * 16 + g + 8 * (e >> 1), col = nb * 8 + 2 * t + (e & 1);
+                atomicAdd(grads + base + row * kMlpH + col, acc[mb][nb][e]);
+            }
+}
+
+__global__ void __launch_bounds__(128, 1) k_mlp_train_tc(const float* __restrict__ params,
+                                                         const float* __restrict__ X, const float* __restrict__ Y,
+                                                         int64_t n, float* __restrict__ grads,
+                                                         float* __restrict__ loss) {
+    extern __shared__ __align__(16) unsigned char mlp_smem[];
+    MlpTrainSmem& S = *reinterpret_cast<MlpTrainSmem*>(mlp_smem);
+    for (int i = threadIdx.x; i < kMlpF * kMlpH; i += blockDim.x) {
+        const int in = i / kMlpH, out = i % kMlpH;
+        S.w1t[out][in] = __float2bfloat16_rn(params[MlpLayout::W1 + i]);
+    }
+    for (int i = threadIdx.x; i < kMlpH * kMlpH; i += blockDim.x) {
+        const int in = i / kMlpH, out = i % kMlpH;
+        const __nv_bfloat16 v = __float2bfloat16_rn(params[MlpLayout::W2 + i]);
+        S.w2t[out][in] = v;
+        S.w2n[in][out] = v;
+    }
+    for (int i = threadIdx.x; i < kMlpH; i += blockDim.x) {
+        S.b1[i] = params[MlpLayout::B1 + i];
+        S.b2[i] = params[MlpLayout::B2 + i];
+        S.w3[i] = bf16r(params[MlpLayout::W3 + i]);
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    MlpTrainSmem::Warp& T = S.w[warp];
+    const float b3 = params[MlpLayout::B3];
+    const float inv_n = 1.0f / (float)n;
+    for (int i = lane; i < 3 * kMlpH; i += 32) (&T.sums[0][0])[i] = 0.0f;
+    __syncwarp();
+    float db3 = 0.0f, lsum = 0.0f;
+    for (int64_t chunk = blockIdx.x;; chunk += gridDim.x) {
+        const int64_t q0 = (chunk * 4 + warp) * 32;
+        if (q0 >= n) break;
+        {
+            const int64_t r = q0 + lane;
+            const bool valid = r < n;
+#pragma unroll 8
+            for (int j = 0; j < kMlpF; ++j) {
+                const __nv_bfloat16 b = __float2bfloat16_rn(valid ? __ldg(X + r * kMlpF + j) : 0.0f);
+                T.x[lane][j] = b;
+                T.xt[j][lane] = b;
+            }
+        }
+        __syncwarp();
+        float acc[2][8][4];
+        mma_layer<kMlpF>(T.x, S.w1t, lane, acc);
+#pragma unroll
+        for (int mb = 0; mb < 2; ++mb)
+#pragma unroll
+            for (int nb = 0; nb < 8; ++nb)
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int row = mb * 16 + g + 8 * (e >> 1), col = nb * 8 + 2 * t + (e & 1);
+                    const __nv_bfloat16 h = __float2bfloat16_rn(fmaxf(acc[mb][nb][e] + S.b1[col], 0.0f));
+                    T.h1[row][col] = h;
+                    T.h1t[col][row] = h;
+                }
+        __syncwarp();
+        mma_layer<kMlpH>(T.h1, S.w2t, lane, acc);
+        float y[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
+#pragma unroll
+        for (int mb = 0; mb < 2; ++mb)
+#pragma unroll
+            for (int nb = 0; nb < 8; ++nb)
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int col = nb * 8 + 2 * t + (e & 1);
+                    const float h2 = bf16r(fmaxf(acc[mb][nb][e] + S.b2[col], 0.0f));
+                    acc[mb][nb][e] = h2;
+                    y[mb][e >> 1] = fmaf(h2, S.w3[col], y[mb][e >> 1]);
+                }
+        float dy[2][2];
+#pragma unroll
+        for (int mb = 0; mb < 2; ++mb)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                float v = y[mb][h];
+                v += __shfl_xor_sync(FULL, v, 1);
+                v += __shfl_xor_sync(FULL, v, 2);
+                const int64_t o = q0 + mb * 16 + g + 8 * h;
+                const float err = o < n ? v + b3 - __ldg(Y + o) : 0.0f;
+                dy[mb][h] = 2.0f * err * inv_n;
+                if (t == 0) {
+                    lsum += err * err * inv_n;
+                    db3 += dy[mb][h];
+                }
+            }
+        // dh2 = (h2 > 0) * dy * w3; w3 and b2 gradients (per lane: columns nb * 8 + 2t + b)
+        float db2[16], dw3[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) db2[i] = dw3[i] = 0.0f;
+#pragma unroll
+        for (int mb = 0; mb < 2; ++mb)
+#pragma unroll
+            for (int nb = 0; nb < 8; ++nb)
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int row = mb * 16 + g + 8 * (e >> 1), col = nb * 8 + 2 * t + (e & 1);
+                    const float h2 = acc[mb][nb][e], d = dy[mb][e >> 1];
+                    const float d2 = h2 > 0.0f ? d * S.w3[col] : 0.0f;
+                    db2[nb * 2 + (e & 1)] += d2;
+                    dw3[nb * 2 + (e & 1)] = fmaf(d, h2, dw3[nb * 2 + (e & 1)]);
+                    const __nv_bfloat16 b = __float2bfloat16_rn(d2);
+                    T.d2[row][col] = b;
+                    T.d2t[col][row] = b;
+                }
+        add_columns(db2, T.sums[1], lane);
+        add_columns(dw3, T.sums[2], lane);
+        __syncwarp();
+        // dh1 = (h1 > 0) * (dh2 W2^T)
+        mma_layer<kMlpH>(T.d2, S.w2n, lane, acc);
+        float db1[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) db1[i] = 0.0f;
+#pragma unroll
+        for (int mb = 0; mb < 2; ++mb)
+#pragma unroll
+            for (int nb = 0; nb < 8; ++nb)
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int row = mb * 16 + g + 8 * (e >> 1), col = nb * 8 + 2 * t + (e & 1);
+                    const float d1 = __bfloat162float(T.h1[row][col]) > 0.0f ? acc[mb][nb][e] : 0.0f;
+                    db1[nb * 2 + (e & 1)] += d1;
+                    T.d1t[col][row] = __float2bfloat16_rn(d1);
+                }
+        add_columns(db1, T.sums[0], lane);
+        __syncwarp();
+        // weight gradients of these 32 rows
+        mma_layer<32>(T.xt, T.d1t, lane, acc);
+        add_tile(grads, MlpLayout::W1, 0, acc, lane);
+        mma_layer<32>(T.h1t, T.d2t, lane, acc);
+        add_tile(grads, MlpLayout::W2, 0, acc, lane);
+        mma_layer<32>(T.h1t + 32, T.d2t, lane, acc);
+        add_tile(grads, MlpLayout::W2, 32, acc, lane);
+        __syncwarp();  // this warp's tiles are rewritten by its next chunk
+    }
+    // this warp's column sums: one reduction per column
+    __syncwarp();
+    for (int i = lane; i < kMlpH; i += 32) {
+        atomicAdd(grads + MlpLayout::B1 + i, T.sums[0][i]);
+        atomicAdd(grads + MlpLayout::B2 + i, T.sums[1][i]);
+        atomicAdd(grads + MlpLayout::W3 + i, T.sums[2][i]);
+    }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        db3 += __shfl_xor_sync(FULL, db3, o);
+        lsum += __shfl_xor_sync(FULL, lsum, o);
+    }
+    if (lane == 0) {
+        atomicAdd(grads + MlpLayout::B3, db3);
+        atomicAdd(loss, lsum);
+    }
+}
+
 inline unsigned blocks_for(int64_t work, int threads) { return (unsigned)((work + threads - 1) / threads); }
 
 }  // namespace
@@ -403,20 +549,21 @@ cudaError_t enqueue_mlp_forward(const float* params, const float* X, int64_t n, 
     return cudaGetLastError();
 }
 
-cudaError_t enqueue_mlp_grad(const float* params, const float* X, const float* y, int64_t n, MlpWork& w, float* grads,
-                             float* loss, cudaStream_t s) {
+cudaError_t enqueue_mlp_grad(const float* params, const float* X, const float* y, int64_t n, MlpWork& /*w*/,
+                             float* grads, float* loss, cudaStream_t s) {
     cudaMemsetAsync(grads, 0, sizeof(float) * kMlpParams, s);
     cudaMemsetAsync(loss, 0, sizeof(float), s);
     if (n <= 0) return cudaGetLastError();
-    k_mlp_forward<<<blocks_for(n, 128), 128, 0, s>>>(params, X, n, w.yhat, w.h1, w.h2);
-    k_mlp_backward_rows<<<blocks_for(n, 128), 128, 0, s>>>(params, w.yhat, y, w.h1, w.h2, n, w.dy, w.dh1, w.dh2, grads,
-                                                           loss);
-    const unsigned ysplit = (unsigned)min64(64, (n + 255) / 256);
-    k_mlp_outer<<<dim3(blocks_for(kMlpF * kMlpH, 256), ysplit), 256, 0, s>>>(X, kMlpF, w.dh1, kMlpH, n, true,
-                                                                            grads + MlpLayout::W1);
-    k_mlp_outer<<<dim3(blocks_for(kMlpH * kMlpH, 256), ysplit), 256, 0, s>>>(w.h1, kMlpH, w.dh2, kMlpH, n, false,
-                                                                            grads + MlpLayout::W2);
-    k_mlp_outer<<<dim3(1, ysplit), 256, 0, s>>>(w.h2, kMlpH, w.dy, 1, n, false, grads + MlpLayout::W3);
+    constexpr int smem = (int)sizeof(MlpTrainSmem);
+    cudaError_t e = cudaFuncSetAttribute(k_mlp_train_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 0;
+    e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    const int64_t want = (n + 127) / 128;  // 4 warps x 32 rows per block and pass
+    const unsigned blocks = (unsigned)(want < sms ? want : (sms > 0 ? sms : 1));
+    k_mlp_train_tc<<<blocks, 128, smem, s>>>(params, X, y, n, grads, loss);
     return cudaGetLastError();
 }
 

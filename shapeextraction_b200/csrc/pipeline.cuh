@@ -191,6 +191,10 @@ struct QueryParams {
     int lut_shift = 0;
     int cell_pmax = 0;
     int cell_span = 3;
+    // persistent batch launches: resident blocks per SM (0: as many as fit)
+    // and warps per block (0: the per-k default; 2 or 4)
+    int batch_blocks_per_sm = 0;
+    int batch_warps_per_block = 0;
 };
 
 // Code-range table of a build for the learned cell scan: lut[j] = the number

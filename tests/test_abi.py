@@ -44,7 +44,7 @@ def test_options_defaults(native):
     assert tuple(o.viewpoint) == (0.0, 0.0, 0.0)
     assert o.search_compat == 0 and o.learned == 0 and o.batch_graph == 1
     assert o.leaf_bucket == 96 and o.seed_halo == -1  # 96-point buckets; halo picked per k
-    assert ctypes.sizeof(o) == 88  # sizeof(se_options) in C: 19 four-byte fields, a pointer, 4 B padding
+    assert ctypes.sizeof(o) == 104  # sizeof(se_options) in C: 23 four-byte fields, a pointer, 4 B padding
     assert L.se_abi_version() == 2
     assert L.se_status_string(5) == b"SE_ERR_NONFINITE"
 
@@ -84,10 +84,14 @@ def test_create_validates_options_before_the_device(native):
         return L.se_create(ctypes.byref(h), ctypes.byref(o))
 
     for bad in ({"leaf_bucket": 129}, {"leaf_bucket": -1}, {"seed_halo": 49}, {"code_bits": 32},
-                {"debug_wait_limit": -1}, {"debug_inject": 8}):
+                {"debug_wait_limit": -1}, {"debug_inject": 8}, {"learned_cell_scan": 2}, {"cell_span": 1},
+                {"cell_span": 5}, {"cell_max_points": -1}, {"batch_lanes": 17}, {"batch_lane_min_points": -1},
+                {"batch_blocks_per_sm": 33}, {"batch_warps_per_block": 3}):
         assert create(**bad) == 1, bad
     for ok in ({"leaf_bucket": 128}, {"leaf_bucket": 1}, {"leaf_bucket": 0}, {"seed_halo": 48},
-               {"debug_wait_limit": 100}, {"debug_inject": 7}):
+               {"debug_wait_limit": 100}, {"debug_inject": 7}, {"learned_cell_scan": 1}, {"cell_span": 4},
+               {"batch_lanes": 16}, {"batch_lane_min_points": 1000}, {"batch_blocks_per_sm": 2},
+               {"batch_warps_per_block": 2}, {"batch_warps_per_block": 4}):
         assert create(**ok) == 2, ok  # valid options: fails only at the missing device (SE_ERR_CUDA)
 
 

@@ -50,11 +50,18 @@ def test_gpu_forward_and_grad_match_oracle(native, oracle):
         loss, g = c.mlp_grad(X, y)
     yo, lo, go = oracle.mlp_grad(p, X, y, round_bf16=True)
     assert np.array_equal(yh.astype(np.float64), yo)  # same roundings, same fmaf order
-    assert abs(loss - lo) <= 1e-5 * abs(lo)
-    rel = np.linalg.norm(g - go) / np.linalg.norm(go)
-    assert rel < 1e-5, rel
-    big = np.abs(go) > 1e-3 * np.abs(go).max()
-    assert np.max(np.abs(g[big] - go[big]) / np.abs(go[big])) < 1e-3
+    # The gradient comes from the tensor-core training step: its FP32 sums run
+    # in the mma order (an activation can round to the neighbouring BF16
+    # value), and dh1, dh2 enter the products in BF16, which the oracle's mode
+    # 2 restates.
+    _, lo2, go2 = oracle.mlp_grad(p, X, y, round_bf16=2)
+    assert abs(loss - lo2) <= 1e-4 * abs(lo2)
+    rel = np.linalg.norm(g - go2) / np.linalg.norm(go2)
+    assert rel < 2e-3, rel
+    big = np.abs(go2) > 1e-2 * np.abs(go2).max()
+    assert np.max(np.abs(g[big] - go2[big]) / np.abs(go2[big])) < 2e-2
+    # and it stays close to the gradient without the BF16 rounding of dh
+    assert np.linalg.norm(g - go) / np.linalg.norm(go) < 1e-2
 
 
 @pytest.mark.gpu

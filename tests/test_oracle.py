@@ -192,3 +192,19 @@ def test_knn_fewer_points_than_k(oracle):
     pts = np.array([[0, 0, 0], [1, 0, 0], [0, 2, 0]], np.float32)
     idx, d2 = oracle.knn_exact(pts, pts, 5)
     assert list(idx[0]) == [0, 1, 2, 0, 0]
+
+
+def test_mlp_grad_modes_agree_to_bf16_rounding(oracle):
+    """The oracle's gradient modes (FP64, BF16 forward, BF16 forward with
+    BF16 dh as the tensor-core training step) differ only by rounding."""
+    rng = np.random.default_rng(4)
+    p = rng.normal(0, 0.2, oracle.MLP_PARAMS).astype(np.float32)
+    X = rng.uniform(-1, 1, (400, 32)).astype(np.float32)
+    y = rng.uniform(-8, 0, 400).astype(np.float32)
+    _, l0, g0 = oracle.mlp_grad(p, X, y, round_bf16=False)
+    _, l1, g1 = oracle.mlp_grad(p, X, y, round_bf16=True)
+    _, l2, g2 = oracle.mlp_grad(p, X, y, round_bf16=2)
+    assert l1 == l2  # the forward is the same in both BF16 modes
+    assert np.linalg.norm(g2 - g1) / np.linalg.norm(g1) < 1e-2
+    assert np.linalg.norm(g1 - g0) / np.linalg.norm(g0) < 5e-2
+    assert not np.array_equal(g1, g2)
