@@ -296,6 +296,10 @@ def run_ours(a):
         return sum(s.elapsed_time(e) for s, e in ev)
 
     def measure():
+        # the clock sampler starts before the warm-up so that its first
+        # samples (nvidia-smi needs a moment to start) fall under load
+        clk = Clocks(local)
+        clk.start()
         for _ in range(a.warmup):
             step_device()
             step_e2e()
@@ -303,8 +307,6 @@ def run_ours(a):
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
-        clk = Clocks(local)
-        clk.start()
         profs = []
         ms_dev = timed(step_device, a.steps, profs)
         stats = ctx.stats()
@@ -508,14 +510,14 @@ def run_batch(a):
 
     step_dev = lambda: ctx.normals_batch(tuple(dev), (ks, offsets), out=out_dev)  # noqa: E731
     step_e2e = lambda: ctx.normals_batch(tuple(host), (ks, offsets), out=out_host)  # noqa: E731
+    clk = Clocks(local)
+    clk.start()
     for _ in range(a.warmup):
         step_dev()
         step_e2e()
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    clk = Clocks(local)
-    clk.start()
     ms_dev = timed(step_dev, a.steps)
     ms_e2e = timed(step_e2e, a.steps)
     clocks = clk.stop()
@@ -766,7 +768,7 @@ def relaunch(a, argv):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="precision_20M_k16")

@@ -299,6 +299,12 @@ SE_API int se_mlp_params(se_ctx* ctx, float* params, int set, int mem);
 SE_API int se_mlp_enable(se_ctx* ctx, int learned, int skip_seed);
 /* Log-margin added to predictions to make them upper bounds. */
 SE_API int se_mlp_set_margin(se_ctx* ctx, float margin_log2);
+/* Training loss of se_mlp_train and se_mlp_grad: quantile 0 (the default) is
+ * the mean squared error of log2(r_k^2 / range^2); a quantile in (0, 1) is
+ * the pinball loss of that quantile, so that the network predicts a per-point
+ * upper bound (the margin then covers only what it still misses). No
+ * counterpart in the reference. */
+SE_API int se_mlp_set_loss(se_ctx* ctx, float quantile);
 /* Forward pass of the training path (CUDA cores): out[n] = y-hat. */
 SE_API int se_mlp_forward(se_ctx* ctx, const float* features, int64_t n, float* out, int mem);
 /* Tensor-core inference fused with the features, on tree points

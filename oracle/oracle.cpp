@@ -836,8 +836,8 @@ static float bf16_round(float v) {
     return r;
 }
 
-int or_mlp_grad(const float* params, const float* X, const float* y, int64_t n, int round_bf16, double* yhat_out,
-                double* grads, double* loss_out) {
+int or_mlp_grad(const float* params, const float* X, const float* y, int64_t n, int round_bf16, double tau,
+                double* yhat_out, double* grads, double* loss_out) {
     constexpr int F = 32, H = 64;
     constexpr int W1 = 0, B1 = W1 + F * H, W2 = B1 + H, B2 = W2 + H * H, W3 = B2 + H, B3 = W3 + H, NP = B3 + 1;
     std::vector<double> g(NP, 0.0);
@@ -878,8 +878,14 @@ int or_mlp_grad(const float* params, const float* X, const float* y, int64_t n, 
         }
         if (yhat_out) yhat_out[r] = yh;
         const double e = yh - (double)y[r];
-        loss += e * e / (double)n;
-        const double dy = 2.0 * e / (double)n;
+        double dy;
+        if (tau > 0.0) {  // pinball loss of quantile tau
+            loss += (e > 0 ? (1.0 - tau) * e : -tau * e) / (double)n;
+            dy = (e > 0 ? 1.0 - tau : (e < 0 ? -tau : 0.0)) / (double)n;
+        } else {          // mean squared error
+            loss += e * e / (double)n;
+            dy = 2.0 * e / (double)n;
+        }
         g[B3] += dy;
         // round_bf16 == 2 restates the tensor-core training step (k_mlp_train_tc):
         // dh2 and dh1 enter the weight gradients, and dh2 the product that

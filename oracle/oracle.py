@@ -60,7 +60,7 @@ def lib():
             "or_cov_ref_f32": (None, [P, P, i64, i32, P]),
             "or_octree_check": (i32, [P, i64, P, i64, i32, i32, P]),
             "or_pipeline_reference": (i64, [P, P, P, i64, i32, P]),
-            "or_mlp_grad": (i32, [P, P, P, i64, i32, P, P, P]),
+            "or_mlp_grad": (i32, [P, P, P, i64, i32, ctypes.c_double, P, P, P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(_lib, name)
@@ -211,12 +211,13 @@ def pipeline_reference(x, y, z, k):
 MLP_PARAMS = 6337
 
 
-def mlp_grad(params, X, y, round_bf16=True):
+def mlp_grad(params, X, y, round_bf16=True, quantile=0.0):
     """(yhat, loss, grads) of the learned-radius MLP's mean squared error.
     round_bf16: False (FP64 throughout), True (BF16 weights, inputs and
     activations with FP32 accumulation, as the GPU's forward), or 2 (that,
     plus the BF16 rounding of dh2 and dh1 that the tensor-core training step
-    applies before its products)."""
+    applies before its products). quantile > 0: the pinball loss of that
+    quantile instead of the mean squared error."""
     params = _f32(params)
     X = _f32(X)
     y = _f32(y)
@@ -225,7 +226,7 @@ def mlp_grad(params, X, y, round_bf16=True):
     grads = np.zeros(MLP_PARAMS, np.float64)
     loss = np.zeros(1, np.float64)
     mode = 2 if round_bf16 == 2 else int(bool(round_bf16))
-    lib().or_mlp_grad(_p(params), _p(X), _p(y), n, mode, _p(yhat), _p(grads), _p(loss))
+    lib().or_mlp_grad(_p(params), _p(X), _p(y), n, mode, float(quantile), _p(yhat), _p(grads), _p(loss))
     return yhat, float(loss[0]), grads
 
 

@@ -35,7 +35,7 @@ EXPORTS = [
     "se_get_points", "se_knn_self", "se_knn", "se_normals", "se_get_stats", "se_get_profile", "se_synchronize",
     "se_sort_keys_static", "se_features", "se_mlp_init", "se_mlp_params", "se_mlp_enable", "se_mlp_set_margin", "se_mlp_forward",
     "se_mlp_predict", "se_mlp_grad", "se_mlp_train", "se_mlp_save", "se_mlp_load", "se_normals_batch",
-    "se_get_batch_tuning", "se_set_batch_tuning", "se_tune_batch",
+    "se_get_batch_tuning", "se_set_batch_tuning", "se_tune_batch", "se_mlp_set_loss",
 ]
 MLP_FEATURES = 32
 MLP_PARAMS = 6337
@@ -140,6 +140,7 @@ def lib():
             "se_mlp_params": (i32, [P, P, i32, i32]),
             "se_mlp_enable": (i32, [P, i32, i32]),
             "se_mlp_set_margin": (i32, [P, ctypes.c_float]),
+            "se_mlp_set_loss": (i32, [P, ctypes.c_float]),
             "se_mlp_forward": (i32, [P, P, i64, P, i32]),
             "se_mlp_predict": (i32, [P, i64, i64, P, P, i32]),
             "se_mlp_grad": (i32, [P, P, P, i64, P, P, i32]),
@@ -368,6 +369,10 @@ class Context:
         p = np.ascontiguousarray(params, np.float32)
         assert p.size == MLP_PARAMS
         self._check(lib().se_mlp_params(self._h, _ptr(p)[0], 1, SE_MEM_HOST), "se_mlp_params")
+
+    def mlp_set_loss(self, quantile=0.0):
+        """Training loss: 0 = squared error, q in (0, 1) = pinball loss of quantile q."""
+        self._check(lib().se_mlp_set_loss(self._h, float(quantile)), "se_mlp_set_loss")
 
     def mlp_set_margin(self, margin):
         self._check(lib().se_mlp_set_margin(self._h, float(margin)), "se_mlp_set_margin")

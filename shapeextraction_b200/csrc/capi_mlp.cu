@@ -140,6 +140,14 @@ int se_mlp_enable(se_ctx* c, int learned, int skip_seed) {
     return SE_OK;
 }
 
+int se_mlp_set_loss(se_ctx* c, float quantile) {
+    if (!c) return SE_ERR_INVALID_ARG;
+    if (!(quantile == 0.0f || (quantile > 0.0f && quantile < 1.0f)))
+        return fail(c, SE_ERR_INVALID_ARG, "quantile must be 0 (squared error) or in (0, 1)");
+    c->mlp_tau = quantile;
+    return SE_OK;
+}
+
 int se_mlp_set_margin(se_ctx* c, float margin_log2) {
     if (!c) return SE_ERR_INVALID_ARG;
     if (!(margin_log2 > -64.0f && margin_log2 < 64.0f)) return fail(c, SE_ERR_INVALID_ARG, "margin out of range");
@@ -202,7 +210,7 @@ int se_mlp_grad(se_ctx* c, const float* features, const float* targets, int64_t 
     const float *X, *Y;
     if (int rc = stage_in(c, features, n * kMlpF, mem, 0, n * kMlpF + n, &X)) return rc;
     if (int rc = stage_in(c, targets, n, mem, n * kMlpF, n * kMlpF + n, &Y)) return rc;
-    SE_CUDA(c, enqueue_mlp_grad(c->mlp, X, Y, n, c->mw, c->mlp_g, c->mlp_loss, c->stream), "launch grad");
+    SE_CUDA(c, enqueue_mlp_grad(c->mlp, X, Y, n, c->mlp_tau, c->mw, c->mlp_g, c->mlp_loss, c->stream), "launch grad");
     const cudaMemcpyKind k = mem == SE_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
     if (grads) SE_CUDA(c, cudaMemcpyAsync(grads, c->mlp_g, sizeof(float) * kMlpParams, k, c->stream), "copy grads");
     if (loss) SE_CUDA(c, cudaMemcpyAsync(loss, c->mlp_loss, sizeof(float), k, c->stream), "copy loss");
@@ -230,7 +238,7 @@ int se_mlp_train(se_ctx* c, const float* features, const float* targets, int64_t
     int64_t row = 0;
     for (int it = 0; it < steps; ++it) {
         if (row + batch > n) row = 0;
-        SE_CUDA(c, enqueue_mlp_grad(c->mlp, X + row * kMlpF, Y + row, batch, c->mw, c->mlp_g,
+        SE_CUDA(c, enqueue_mlp_grad(c->mlp, X + row * kMlpF, Y + row, batch, c->mlp_tau, c->mw, c->mlp_g,
                                     dloss ? dloss + it : c->mlp_loss, c->stream),
                 "launch grad");
         SE_CUDA(c, enqueue_adam(c->mlp, c->mlp_g, c->mlp_m, c->mlp_v, lr, ++c->mlp_step, c->stream), "launch adam");

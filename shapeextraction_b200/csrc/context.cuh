@@ -71,6 +71,7 @@ struct se_ctx {
     float* mlp_loss = nullptr;
     int mlp_step = 0;
     float mlp_margin = 0.0f;
+    float mlp_tau = 0.0f;  // training loss: 0 squared error, else the pinball loss of this quantile
     bool mlp_ready = false;
     MlpWork mw{};
     int64_t mw_cap = 0;

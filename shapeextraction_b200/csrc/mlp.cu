@@ -300,7 +300,8 @@ __global__ void __launch_bounds__(128) k_predict_radius(const float* __restrict_
 
 // ---------------------------------------------------------------------------
 // Training step on the tensor cores: forward, backward and weight gradients of
-// the mean squared error for one batch in one kernel. A warp takes 32 rows at
+// the loss (mean squared error, or with tau > 0 the pinball loss of quantile
+// tau) for one batch in one kernel. A warp takes 32 rows at
 // a time: both hidden layers, dh1 = (h1 > 0) * (dh2 W2^T) and the weight
 // gradients dW1 = X^T dh1 and dW2 = h1^T dh2 (K = the 32 rows) are
 // mma.sync.m16n8k16 products over BF16 tiles in shared memory (row-major tiles
@@ -361,7 +362,7 @@ __device__ __forceinline__ void add_tile(float* __restrict__ grads, int base, in
 
 __global__ void __launch_bounds__(128, 1) k_mlp_train_tc(const float* __restrict__ params,
                                                          const float* __restrict__ X, const float* __restrict__ Y,
-                                                         int64_t n, float* __restrict__ grads,
+                                                         int64_t n, float tau, float* __restrict__ grads,
                                                          float* __restrict__ loss) {
     extern __shared__ __align__(16) unsigned char mlp_smem[];
     MlpTrainSmem& S = *reinterpret_cast<MlpTrainSmem*>(mlp_smem);
@@ -440,9 +441,16 @@ __global__ void __launch_bounds__(128, 1) k_mlp_train_tc(const float* __restrict
                 v += __shfl_xor_sync(FULL, v, 2);
                 const int64_t o = q0 + mb * 16 + g + 8 * h;
                 const float err = o < n ? v + b3 - __ldg(Y + o) : 0.0f;
-                dy[mb][h] = 2.0f * err * inv_n;
+                float l;
+                if (tau > 0.0f) {  // pinball loss at quantile tau: tau (y - yhat)+ + (1 - tau) (yhat - y)+
+                    dy[mb][h] = (err > 0.0f ? 1.0f - tau : (err < 0.0f ? -tau : 0.0f)) * inv_n;
+                    l = (err > 0.0f ? (1.0f - tau) * err : -tau * err) * inv_n;
+                } else {  // mean squared error
+                    dy[mb][h] = 2.0f * err * inv_n;
+                    l = err * err * inv_n;
+                }
                 if (t == 0) {
-                    lsum += err * err * inv_n;
+                    lsum += l;
                     db3 += dy[mb][h];
                 }
             }
@@ -549,8 +557,8 @@ cudaError_t enqueue_mlp_forward(const float* params, const float* X, int64_t n, 
     return cudaGetLastError();
 }
 
-cudaError_t enqueue_mlp_grad(const float* params, const float* X, const float* y, int64_t n, MlpWork& /*w*/,
-                             float* grads, float* loss, cudaStream_t s) {
+cudaError_t enqueue_mlp_grad(const float* params, const float* X, const float* y, int64_t n, float tau,
+                             MlpWork& /*w*/, float* grads, float* loss, cudaStream_t s) {
     cudaMemsetAsync(grads, 0, sizeof(float) * kMlpParams, s);
     cudaMemsetAsync(loss, 0, sizeof(float), s);
     if (n <= 0) return cudaGetLastError();
@@ -563,7 +571,7 @@ cudaError_t enqueue_mlp_grad(const float* params, const float* X, const float* y
     if (e != cudaSuccess) return e;
     const int64_t want = (n + 127) / 128;  // 4 warps x 32 rows per block and pass
     const unsigned blocks = (unsigned)(want < sms ? want : (sms > 0 ? sms : 1));
-    k_mlp_train_tc<<<blocks, 128, smem, s>>>(params, X, y, n, grads, loss);
+    k_mlp_train_tc<<<blocks, 128, smem, s>>>(params, X, y, n, tau, grads, loss);
     return cudaGetLastError();
 }
 

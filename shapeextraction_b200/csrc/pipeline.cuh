@@ -154,8 +154,8 @@ cudaError_t enqueue_predict_radius(const BuildBufs& b, const float* params, floa
                                    int64_t start, int64_t count, float* r2_out, float* yhat_out, cudaStream_t s);
 cudaError_t enqueue_mlp_forward(const float* params, const float* X, int64_t n, float* yhat, float* h1, float* h2,
                                 cudaStream_t s);
-cudaError_t enqueue_mlp_grad(const float* params, const float* X, const float* y, int64_t n, MlpWork& w, float* grads,
-                             float* loss, cudaStream_t s);
+cudaError_t enqueue_mlp_grad(const float* params, const float* X, const float* y, int64_t n, float tau, MlpWork& w,
+                             float* grads, float* loss, cudaStream_t s);
 cudaError_t enqueue_adam(float* params, const float* grads, float* m, float* v, float lr, int step, cudaStream_t s);
 
 // Sort n 64-bit keys in place in `keys` (ascending) with the onesweep passes;

@@ -43,13 +43,17 @@ def _sample(ctx: Context, k: int, max_rows: int, rng) -> tuple[np.ndarray, np.nd
 
 
 def train_radius_model(ctx: Context, k: int, steps: int = 1500, batch: int = 8192, lr: float = 2e-3, seed: int = 0,
-                       quantile: float = 0.995, max_rows: int = 1_000_000) -> dict:
+                       quantile: float = 0.995, max_rows: int = 1_000_000, pinball: float = 0.0,
+                       pinball_steps: int = 500) -> dict:
     """Train the context's model on its own built cloud (the held-out cloud)
     and calibrate the margin at the `quantile` of the training residuals.
     A warp searches again whenever one of its 32 lanes misses, so misses cost
     far more than a slightly looser bound: 0.995 measured best on surface,
     mixture and precision-mix clouds (0.99 and 0.999 were 1-4% slower).
-    Returns the losses and the calibration."""
+    With pinball in (0, 1) the squared-error training is followed by
+    pinball_steps steps of the pinball loss of that quantile, so that the
+    network predicts a per-point upper bound and the global margin covers
+    only the rest. Returns the losses and the calibration."""
     rng = np.random.default_rng(seed)
     X, y = _sample(ctx, k, max_rows, rng)
     perm = rng.permutation(y.size)
@@ -58,7 +62,12 @@ def train_radius_model(ctx: Context, k: int, steps: int = 1500, batch: int = 819
     p = ctx.mlp_params()
     p[B3] = float(ys.mean())
     ctx.mlp_params(p)
+    ctx.mlp_set_loss(0.0)
     losses = ctx.mlp_train(Xs, ys, steps, batch, lr)
+    if pinball > 0.0 and pinball_steps > 0:
+        ctx.mlp_set_loss(pinball)
+        losses = np.concatenate([losses, ctx.mlp_train(Xs, ys, pinball_steps, batch, lr * 0.5)])
+        ctx.mlp_set_loss(0.0)
     # calibrate with the training forward over the same rows; the tensor-core
     # path that queries use differs from it by far less than the 0.02 added
     yhat = np.concatenate([ctx.mlp_forward(Xs[i:i + 1_000_000]) for i in range(0, ys.size, 1_000_000)])
@@ -66,7 +75,7 @@ def train_radius_model(ctx: Context, k: int, steps: int = 1500, batch: int = 819
     margin = float(np.quantile(res, quantile)) + 0.02
     ctx.mlp_set_margin(margin)
     return {"losses": losses, "margin": margin, "quantile": quantile, "rows": int(ys.size),
-            "residual_std": float(res.std()), "target_mean": float(y.mean())}
+            "residual_std": float(res.std()), "target_mean": float(y.mean()), "pinball": pinball}
 
 
 def transfer(src: Context, dst: Context, margin: float) -> None:

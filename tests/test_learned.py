@@ -65,6 +65,25 @@ def test_gpu_forward_and_grad_match_oracle(native, oracle):
 
 
 @pytest.mark.gpu
+def test_pinball_gradient_matches_oracle(native, oracle):
+    """The quantile (pinball) loss of se_mlp_set_loss, against the oracle's
+    restatement with the same roundings."""
+    rng = np.random.default_rng(6)
+    p = _rand_params(4)
+    X = rng.uniform(-1, 1, (3000, 32)).astype(np.float32)
+    y = rng.uniform(-8, 0, 3000).astype(np.float32)
+    with native.Context() as c:
+        c.mlp_params(p)
+        c.mlp_set_loss(0.9)
+        loss, g = c.mlp_grad(X, y)
+        with pytest.raises(native.ShapexError):
+            c.mlp_set_loss(1.0)
+    _, lo, go = oracle.mlp_grad(p, X, y, round_bf16=2, quantile=0.9)
+    assert abs(loss - lo) <= 1e-4 * abs(lo)
+    assert np.linalg.norm(g - go) / np.linalg.norm(go) < 2e-3
+
+
+@pytest.mark.gpu
 def test_tensor_core_inference_matches_training_forward(native):
     x, y, z = synth.scene(50_000, 5)
     with native.Context() as c:
