@@ -200,11 +200,17 @@ def _dist():
     return world, rank, local
 
 
-def _init_dist(world, local, backend="nccl"):
+def _init_dist(world, local, backend="nccl", single=False):
     """One process group per run, short timeout (ranks that wait on each
-    other end with an error instead of hanging)."""
-    if world <= 1:
+    other end with an error instead of hanging). single: a one-rank group
+    too (the sharded path calls the collectives whatever the rank count)."""
+    if world <= 1 and not single:
         return
+    if world <= 1:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        os.environ.setdefault("MASTER_PORT", str(_free_port()))
+        os.environ.setdefault("RANK", "0")
+        os.environ.setdefault("WORLD_SIZE", "1")
     from datetime import timedelta
 
     import torch
@@ -237,9 +243,9 @@ def run_ours(a):
 
     world, rank, local = _dist()
     torch.cuda.set_device(local)
-    _init_dist(world, local)
-    dev = torch.device("cuda", local)
     sharded = a.mode == "sharded"
+    _init_dist(world, local, single=sharded)
+    dev = torch.device("cuda", local)
     wl = _workloads(a.points)[a.workload]
     k = wl["k"]
     # replicas: one cloud per rank; sharded: rank 0's cloud, broadcast each step
@@ -459,7 +465,7 @@ def run_ours(a):
         }
         print(json.dumps(line), flush=True)
     ctx.close()
-    if world > 1:
+    if dist.is_initialized():
         dist.barrier()
         dist.destroy_process_group()
 
