@@ -36,11 +36,13 @@ namespace {
 constexpr int kStackDepth = 96;
 // Per-k tile shape, measured on B200 (2M scene and 5M mixture clouds): small
 // lists leave registers for more resident warps, which pays for itself up to
-// k = 16. The 24- and 32-key lists need their registers (about 144), so they
-// keep the larger buffer and run in 2-warp blocks: 7 resident blocks (14
-// warps) where 4-warp blocks fit only 3 (12 warps); k = 32 ran 2.7% faster.
-// min_blocks stays at 6 so that ptxas does not cap the registers (a cap of
-// 7 x 64 threads forced 128 registers and spills). Registers, not shared
+// k = 16. The 24- and 32-key lists need more registers, so they keep the
+// larger buffer and run in 2-warp blocks: 7 resident blocks (14 warps) where
+// 4-warp blocks fit only 3 (12 warps); k = 32 ran 2.7% faster. k = 24 fits
+// 128 registers without spills and is asked for 8 blocks (16 warps): at 130
+// registers (7 blocks) it ran 11% slower on the 2M scene. k = 32 asks for 6
+// so that ptxas does not cap its registers (a cap of 7 x 64 threads forced
+// 128 registers and spills). Registers, not shared
 // memory, hold k <= 16 at 5 blocks, so its buffer grew from 48 to 56 slots
 // (fewer flushes; the learned search ran 3% faster). 64 slots shrank the L1
 // cache enough to cost 3-4%.
@@ -49,7 +51,7 @@ struct KnnCfg {
     static constexpr int buf = K <= 8 ? 40 : (K <= 16 ? 56 : 64);  // candidate buffer slots per lane
     static constexpr int threads = K <= 16 ? 128 : 64;              // block size
     static constexpr int warps = threads / 32;
-    static constexpr int min_blocks = K <= 8 ? 6 : (K <= 16 ? 5 : 6);  // resident blocks per SM asked of ptxas
+    static constexpr int min_blocks = K <= 8 ? 6 : (K <= 16 ? 5 : (K <= 24 ? 8 : 6));  // resident blocks per SM asked of ptxas
 };
 constexpr int kMaxHalo = 48;            // seed points on each side of a warp's queries
 constexpr int kWindowMax = 32 + 2 * kMaxHalo;
@@ -195,27 +197,31 @@ struct WarpSmem {
     int32_t buf[B][32];
 };
 
+// Ordered widest first so that the struct packs into 128 bytes: one more
+// padded word (144 bytes) made ptxas give the k = 32 kernels 161-163
+// registers instead of 142, one resident block per SM fewer.
 struct QArgs {
-    int k;
     int64_t start, count, u;
     const float* ext;
     int32_t* out_idx;
     float* out_d2;
     float* out_normals;
+    const float* learned_r2;
+    const uint32_t* cell_lut;  // learned cell scan: code-range table (null: tree walk with the cap)
     float vx, vy, vz;
     float gap;
+    int k;
     int code_bits;
     int bucket;
     int seed_halo;
-    const float* learned_r2;
     int learned_skip_seed;
     int device_count;  // 1: u = count = the build's unique-point count, read on the device (start 0)
     int step_limit;    // > 0: node visits per warp before the walk gives up (test hook)
-    const uint32_t* cell_lut;  // learned cell scan: code-range table (null: tree walk with the cap)
-    int lut_shift;             // per-axis shift of the table's level (bits per axis - level)
-    int cell_pmax;             // cell scan: most points per warp before it falls back to the walk
-    int cell_span;             // cell scan: most cells per axis covering one lane's ball (2..4)
+    int lut_shift;     // per-axis shift of the table's level (bits per axis - level)
+    int cell_pmax;     // cell scan: most points per warp before it falls back to the walk
+    int cell_span;     // cell scan: most cells per axis covering one lane's ball (2..4)
 };
+static_assert(sizeof(QArgs) == 128, "QArgs grew past 128 bytes");
 
 struct Counters {
     int cand = 0, ins = 0, merge = 0, buckets = 0, lmiss = 0, cells = 0, cell_fallback = 0, cell_lookups = 0,
