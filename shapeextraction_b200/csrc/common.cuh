@@ -94,6 +94,28 @@ __device__ __forceinline__ float dist2(float qx, float qy, float qz, float px, f
     return __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
 }
 
+// dist2 for two points at once with sm_100's packed FP32 instructions: each
+// 64-bit operand holds two floats (the first point in the low half), and each
+// half is rounded exactly as the scalar instruction rounds it, so both halves
+// of the result equal dist2 bit for bit. qq* hold the query coordinate twice.
+__device__ __forceinline__ uint64_t dist2_pair(uint64_t qqx, uint64_t qqy, uint64_t qqz, uint64_t x, uint64_t y,
+                                               uint64_t z) {
+    uint64_t dx, dy, dz, s;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(dx) : "l"(qqx), "l"(x));
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(dy) : "l"(qqy), "l"(y));
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(dz) : "l"(qqz), "l"(z));
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(s) : "l"(dz), "l"(dz));
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(s) : "l"(dy), "l"(dy), "l"(s));
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(s) : "l"(dx), "l"(dx), "l"(s));
+    return s;
+}
+__device__ __forceinline__ uint64_t twice(float v) {
+    const uint64_t b = __float_as_uint(v);
+    return (b << 32) | b;
+}
+__device__ __forceinline__ float lo_half(uint64_t v) { return __uint_as_float((uint32_t)v); }
+__device__ __forceinline__ float hi_half(uint64_t v) { return __uint_as_float((uint32_t)(v >> 32)); }
+
 // Squared distance from q to a box with the same rounding chain; never larger
 // than dist2 to any point inside the box (rounding is monotonic).
 __device__ __forceinline__ float box_dist2(float qx, float qy, float qz, float lx, float ly, float lz, float hx,

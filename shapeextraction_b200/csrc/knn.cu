@@ -282,24 +282,38 @@ __device__ __forceinline__ void flush(TopK<K, EXACT>& tk, int& bc, WS& W, int la
 // every one whose distance reaches the lane's bound to the lane's buffer.
 // Points of the seed window [w0, w1) are skipped (they were already offered).
 // The caller guarantees that bc + cnt fits the buffer.
+// The points are staged in pairs for dist2_pair: floats [4j, 4j + 4) hold
+// x and y of points 2j and 2j + 1, floats [64 + 2j, 64 + 2j + 2) their z; a
+// slot past cnt holds a NaN x, whose distance passes no bound.
 template <class WS>
 __device__ __forceinline__ void scan_chunk(int32_t first, int cnt, bool need, float qx, float qy, float qz,
                                            float tau, int& bc, WS& W, const float4* __restrict__ pts,
                                            int32_t w0, int32_t w1, int lane) {
-    if (lane < cnt) W.pts[lane] = __ldg(pts + first + lane);
+    float* f = reinterpret_cast<float*>(W.pts);
+    {
+        const float4 p = lane < cnt ? __ldg(pts + first + lane) : make_float4(__int_as_float(0x7fc00000), 0.f, 0.f, 0.f);
+        const int o = 4 * (lane >> 1) + (lane & 1);
+        f[o] = p.x;
+        f[o + 2] = p.y;
+        f[64 + lane] = p.z;
+    }
     __syncwarp();
     if (need) {
+        const uint64_t qqx = twice(qx), qqy = twice(qy), qqz = twice(qz);
         if (first < w1 && first + cnt > w0) {  // overlaps the seed window: skip its points
-            for (int t = 0; t < cnt; ++t) {
-                const float4 p = W.pts[t];
-                const float d = dist2(qx, qy, qz, p.x, p.y, p.z);
+            for (int t = 0; t < cnt; t += 2) {
+                const ulonglong2 xy = *reinterpret_cast<const ulonglong2*>(f + 2 * t);
+                const uint64_t d = dist2_pair(qqx, qqy, qqz, xy.x, xy.y, *reinterpret_cast<const uint64_t*>(f + 64 + t));
                 const int32_t idx = first + t;
-                if (d <= tau && (idx < w0 || idx >= w1)) W.buf[bc++][lane] = idx;
+                if (lo_half(d) <= tau && (idx < w0 || idx >= w1)) W.buf[bc++][lane] = idx;
+                if (hi_half(d) <= tau && (idx + 1 < w0 || idx + 1 >= w1)) W.buf[bc++][lane] = idx + 1;
             }
         } else {
-            for (int t = 0; t < cnt; ++t) {
-                const float4 p = W.pts[t];
-                if (dist2(qx, qy, qz, p.x, p.y, p.z) <= tau) W.buf[bc++][lane] = first + t;
+            for (int t = 0; t < cnt; t += 2) {
+                const ulonglong2 xy = *reinterpret_cast<const ulonglong2*>(f + 2 * t);
+                const uint64_t d = dist2_pair(qqx, qqy, qqz, xy.x, xy.y, *reinterpret_cast<const uint64_t*>(f + 64 + t));
+                if (lo_half(d) <= tau) W.buf[bc++][lane] = first + t;
+                if (hi_half(d) <= tau) W.buf[bc++][lane] = first + t + 1;
             }
         }
     }
