@@ -343,7 +343,7 @@ SE_API int se_mlp_load(se_ctx* ctx, const char* path);
  *   stream before it returns. It must never be called while a stream is being
  *   captured into a CUDA graph. */
 #define SE_STATIC_SORT_MAX_KEYS (1 << 20)
-#define SE_STATIC_SORT_BYTES (8u * (1u << 20) + 256u * 1024u + 20480u)
+#define SE_STATIC_SORT_BYTES (8u * (1u << 20) + 512u * 1024u + 36864u)
 SE_API int se_sort_keys_static(const uint64_t* d_keys_in, uint64_t* d_keys_out, int64_t n, void* stream);
 
 /* Waits for all work queued on the context's stream. */

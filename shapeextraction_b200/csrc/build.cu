@@ -120,13 +120,13 @@ __device__ __forceinline__ void load_bbox(const DevState* st, float& mn, float& 
 
 // ---------------------------------------------------------------------------
 // encode: replaces makeCodes (src/RadixTree.cu:21-39, 244-248); also builds
-// the 8 digit histograms of the onesweep sort in the same pass.
+// the digit histograms of the onesweep sort's passes in the same pass.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_encode(const float* __restrict__ x, const float* __restrict__ y,
                                                 const float* __restrict__ z, int64_t n, int code_bits,
                                                 uint64_t* __restrict__ keys, DevState* st) {
-    __shared__ uint32_t s_h[kSortPasses][256];
-    for (int i = threadIdx.x; i < kSortPasses * 256; i += blockDim.x) (&s_h[0][0])[i] = 0;
+    __shared__ uint32_t s_h[kSortPasses][kSortBins];
+    for (int i = threadIdx.x; i < kSortPasses * kSortBins; i += blockDim.x) (&s_h[0][0])[i] = 0;
     __syncthreads();
     float mn, range;
     load_bbox(st, mn, range);
@@ -140,24 +140,24 @@ __global__ void __launch_bounds__(256) k_encode(const float* __restrict__ x, con
         const uint64_t c = point_to_code(__ldcs(x + i), __ldcs(y + i), __ldcs(z + i), mn, range, code_bits);
         keys[i] = c;
 #pragma unroll
-        for (int p = 0; p < kSortPasses; ++p) atomicAdd(&s_h[p][(c >> (8 * p)) & 255], 1u);
+        for (int p = 0; p < kSortPasses; ++p) atomicAdd(&s_h[p][(c >> (kSortBits * p)) & (kSortBins - 1)], 1u);
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < kSortPasses * 256; i += blockDim.x) {
+    for (int i = threadIdx.x; i < kSortPasses * kSortBins; i += blockDim.x) {
         const uint32_t v = (&s_h[0][0])[i];
         if (v) atomicAdd(&(&st->hist[0][0])[i], v);
     }
 }
 
 // Digit offsets, trivial-pass detection and ping-pong parity, on one block.
-__global__ void __launch_bounds__(256) k_sort_prep(int64_t n, DevState* st) {
-    __shared__ uint32_t s_w[9];
+__global__ void __launch_bounds__(kSortBins) k_sort_prep(int64_t n, DevState* st) {
+    __shared__ uint32_t s_w[kSortBins / 32 + 1];
     __shared__ int s_triv[kSortPasses];
     const int d = threadIdx.x;
     for (int p = 0; p < kSortPasses; ++p) {
         const uint32_t h = st->hist[p][d];
         uint32_t tot;
-        const uint32_t ex = block_excl_scan<256, uint32_t>(h, s_w, &tot);
+        const uint32_t ex = block_excl_scan<kSortBins, uint32_t>(h, s_w, &tot);
         st->digit_off[p][d] = ex;
         if (d == 0) s_triv[p] = 0;
         __syncthreads();
@@ -180,16 +180,23 @@ __global__ void __launch_bounds__(256) k_sort_prep(int64_t n, DevState* st) {
 // "Onesweep: A Faster Least Significant Digit Radix Sort for GPUs", 2022):
 // warp-level multi-split ranking with ballot peer masks, decoupled look-back
 // over per-tile digit counts, scatter through shared memory. Replaces
-// DeviceRadixSort::SortKeys (src/RadixTree.cu:316-337). Stable. Three blocks
-// per SM (40 registers, the whole shared-memory carveout): 17% faster than
-// two on 20M keys, where short-scoreboard and barrier waits dominate.
+// DeviceRadixSort::SortKeys (src/RadixTree.cu:316-337). Stable.
+//
+// 9-bit digits (512 bins, one per thread), so a 63-bit Morton code takes 7
+// passes instead of 8. A tile publishes its digit counts as soon as it has
+// ranked its keys, scatters them into shared memory, and only then reads its
+// predecessors' counts. Three blocks per SM (the whole shared-memory
+// carveout).
 // ---------------------------------------------------------------------------
+constexpr int kSortWarps = kSortThreads / 32;
+static_assert(kSortThreads == kSortBins, "one digit per thread");
+
 struct SortSmem {
-    uint32_t hist[kSortThreads / 32][256];
+    uint32_t hist[kSortWarps][kSortBins];  // per-warp digit counts, then per-warp offsets
     uint64_t keys[kSortTile];
-    uint32_t local_start[256];
-    uint32_t global_base[256];
-    uint32_t scan_w[9];
+    uint32_t local_start[kSortBins];  // first slot of each digit in the tile
+    int32_t goff[kSortBins];          // global position of the digit's run minus local_start
+    uint32_t scan_w[kSortWarps + 1];
     uint32_t tile_id;
 };
 
@@ -203,10 +210,10 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(uint64_t* buf0, ui
     const int parity = st->pass_parity[pass];
     const uint64_t* __restrict__ in = parity ? buf1 : buf0;
     uint64_t* __restrict__ out = parity ? buf0 : buf1;
-    const int shift = 8 * pass;
+    const int shift = kSortBits * pass;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
-    for (int i = tid; i < (kSortThreads / 32) * 256; i += kSortThreads) (&S.hist[0][0])[i] = 0;
+    for (int i = tid; i < kSortWarps * kSortBins; i += kSortThreads) (&S.hist[0][0])[i] = 0;
     if (tid == 0) S.tile_id = atomicAdd(&st->tile_counter[pass], 1u);
     __syncthreads();
     const uint32_t tile = S.tile_id;
@@ -224,13 +231,13 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(uint64_t* buf0, ui
     for (int i = 0; i < kSortIpt; ++i) {
         const int64_t idx = wbase + i * 32 + lane;
         const bool valid = idx < n;
-        const uint32_t d = valid ? (uint32_t)((key[i] >> shift) & 255) : 256u;
-        // lanes holding the same digit: 9 ballots (validity, then the 8 digit
-        // bits), measured slightly faster than __match_any_sync here
+        const uint32_t d = (uint32_t)(key[i] >> shift) & (kSortBins - 1);
+        // lanes holding the same digit: one ballot for validity, one per digit
+        // bit (measured slightly faster than __match_any_sync)
         uint32_t peers = __ballot_sync(0xffffffffu, valid);
         if (!valid) peers = ~peers;
 #pragma unroll
-        for (int bb = 0; bb < 8; ++bb) {
+        for (int bb = 0; bb < kSortBits; ++bb) {
             const uint32_t v = __ballot_sync(0xffffffffu, (d >> bb) & 1u);
             peers &= ((d >> bb) & 1u) ? v : ~v;
         }
@@ -243,62 +250,64 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(uint64_t* buf0, ui
     }
     __syncthreads();
 
-    // per-digit exclusive prefix over warps; tile digit counts
+    // digit `tid`: exclusive prefix over warps and the tile's count, published
+    // at once so that successors' look-backs find it early
+    const int dg = tid;
     uint32_t cnt = 0;
-    if (tid < 256) {
-        for (int w = 0; w < kSortThreads / 32; ++w) {
-            const uint32_t c = S.hist[w][tid];
-            S.hist[w][tid] = cnt;
-            cnt += c;
-        }
+    for (int w = 0; w < kSortWarps; ++w) {
+        const uint32_t c = S.hist[w][dg];
+        S.hist[w][dg] = cnt;
+        cnt += c;
     }
-    // decoupled look-back on digit `tid`
-    uint32_t excl = 0;
-    if (tid < 256) {
-        uint32_t* mine = lookback + (size_t)tile * 256 + tid;
-        if (tile == 0) {
-            if (!stall_first_tile) st_relaxed(mine, LB_PRE | cnt);
-        } else {
-            st_relaxed(mine, LB_AGG | cnt);
-            int64_t p = (int64_t)tile - 1;
-            int spins = 0;
-            while (p >= 0) {
-                const uint32_t v = ld_relaxed(lookback + (size_t)p * 256 + tid);
-                const uint32_t f = v >> 30;
-                if (f == 0) {
-                    if (++spins > spin_limit) { set_err(&st->err, ERRBIT_LOOKBACK); break; }
-                    continue;
-                }
-                excl += v & LB_VAL;
-                if (f == 2) break;
-                --p;
-            }
-            st_relaxed(mine, LB_PRE | (excl + cnt));
-        }
+    if (tile == 0) {
+        if (!stall_first_tile) st_relaxed(lookback + dg, LB_PRE | cnt);
+    } else {
+        st_relaxed(lookback + (size_t)tile * kSortBins + dg, LB_AGG | cnt);
     }
     {
         uint32_t tot;
-        const uint32_t ls = block_excl_scan<kSortThreads, uint32_t>(tid < 256 ? cnt : 0u, S.scan_w, &tot);
-        if (tid < 256) {
-            S.local_start[tid] = ls;
-            S.global_base[tid] = st->digit_off[pass][tid] + excl;
-        }
+        S.local_start[dg] = block_excl_scan<kSortThreads, uint32_t>(cnt, S.scan_w, &tot);
     }
     __syncthreads();
+    // keys into shared memory in digit order
 #pragma unroll
     for (int i = 0; i < kSortIpt; ++i) {
         const int64_t idx = wbase + i * 32 + lane;
         if (idx < n) {
-            const uint32_t d = (uint32_t)((key[i] >> shift) & 255);
+            const uint32_t d = (uint32_t)(key[i] >> shift) & (kSortBins - 1);
             S.keys[S.local_start[d] + S.hist[warp][d] + rank[i]] = key[i];
         }
     }
+    // decoupled look-back on digit `dg`, after the scatter: by then most
+    // predecessors have published (reading them earlier, or several at a time,
+    // measured slower: the polls compete with the tiles still ranking)
+    uint32_t excl = 0;
+    if (tile > 0) {
+        int64_t p = (int64_t)tile - 1;
+        int spins = 0;
+        while (p >= 0) {
+            const uint32_t v = ld_relaxed(lookback + (size_t)p * kSortBins + dg);
+            const uint32_t f = v >> 30;
+            if (f == 0) {
+                if (++spins > spin_limit) {
+                    set_err(&st->err, ERRBIT_LOOKBACK);
+                    break;
+                }
+                continue;
+            }
+            excl += v & LB_VAL;
+            if (f == 2) break;
+            --p;
+        }
+        st_relaxed(lookback + (size_t)tile * kSortBins + dg, LB_PRE | (excl + cnt));
+    }
+    S.goff[dg] = (int32_t)(st->digit_off[pass][dg] + excl) - (int32_t)S.local_start[dg];
     __syncthreads();
     const int tile_n = (int)min64(kSortTile, n - base);
     for (int j = tid; j < tile_n; j += kSortThreads) {
         const uint64_t k = S.keys[j];
-        const uint32_t d = (uint32_t)((k >> shift) & 255);
-        const int64_t pos = (int64_t)S.global_base[d] + (j - (int64_t)S.local_start[d]);
+        const uint32_t d = (uint32_t)(k >> shift) & (kSortBins - 1);
+        const int64_t pos = (int64_t)S.goff[d] + j;
         if (pos >= 0 && pos < n) out[pos] = k;
         else set_err(&st->err, ERRBIT_BOUNDS);
     }
@@ -875,17 +884,17 @@ __global__ void __launch_bounds__(256) k_oct_link(OtNode* __restrict__ nodes, in
 // Digit histograms of given keys (the histogram half of k_encode), for
 // sorting keys that were not produced by k_encode.
 __global__ void __launch_bounds__(256) k_hist_keys(const uint64_t* __restrict__ keys, int64_t n, DevState* st) {
-    __shared__ uint32_t s_h[kSortPasses][256];
-    for (int i = threadIdx.x; i < kSortPasses * 256; i += blockDim.x) (&s_h[0][0])[i] = 0;
+    __shared__ uint32_t s_h[kSortPasses][kSortBins];
+    for (int i = threadIdx.x; i < kSortPasses * kSortBins; i += blockDim.x) (&s_h[0][0])[i] = 0;
     __syncthreads();
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
         const uint64_t c = keys[i];
 #pragma unroll
-        for (int p = 0; p < kSortPasses; ++p) atomicAdd(&s_h[p][(c >> (8 * p)) & 255], 1u);
+        for (int p = 0; p < kSortPasses; ++p) atomicAdd(&s_h[p][(c >> (kSortBits * p)) & (kSortBins - 1)], 1u);
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < kSortPasses * 256; i += blockDim.x) {
+    for (int i = threadIdx.x; i < kSortPasses * kSortBins; i += blockDim.x) {
         const uint32_t v = (&s_h[0][0])[i];
         if (v) atomicAdd(&(&st->hist[0][0])[i], v);
     }
@@ -909,7 +918,7 @@ inline unsigned grid_for(int64_t work, int threads, int64_t cap_blocks) {
 
 }  // namespace
 
-// Onesweep's shared memory (51 KB per block) with the whole carveout for
+// Onesweep's shared memory (68 KB per block) with the whole carveout for
 // shared memory, so that the 3 blocks its registers allow fit on an SM.
 static cudaError_t set_onesweep_attributes() {
     cudaError_t e = cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -927,10 +936,10 @@ cudaError_t enqueue_sort_keys(uint64_t* keys, uint64_t* tmp, int64_t n, uint32_t
     cudaMemsetAsync(st, 0, sizeof(DevState), s);
     if (n <= 0) return cudaGetLastError();
     k_hist_keys<<<grid_for(n, 256, num_sms * 4), 256, 0, s>>>(keys, n, st);
-    k_sort_prep<<<1, 256, 0, s>>>(n, st);
+    k_sort_prep<<<1, kSortBins, 0, s>>>(n, st);
     const int64_t sort_tiles = (n + kSortTile - 1) / kSortTile;
     for (int pass = 0; pass < kSortPasses; ++pass) {
-        cudaMemsetAsync(lookback, 0, sizeof(uint32_t) * 256 * sort_tiles, s);
+        cudaMemsetAsync(lookback, 0, sizeof(uint32_t) * kSortBins * sort_tiles, s);
         k_onesweep<<<(unsigned)sort_tiles, kSortThreads, sizeof(SortSmem), s>>>(keys, tmp, n, pass, lookback, st,
                                                                                  kSpinLimit, 0);
     }
@@ -983,12 +992,12 @@ cudaError_t enqueue_build(const BuildBufs& b, const BuildParams& p, cudaStream_t
     k_bbox<<<grid_for((n + 3) / 4, 256, num_sms * 4), 256, 0, s>>>(b.x, b.y, b.z, n, b.st);
     mark(1);
     k_encode<<<grid_for(n, 256, num_sms * 4), 256, 0, s>>>(b.x, b.y, b.z, n, p.code_bits, b.keys0, b.st);
-    k_sort_prep<<<1, 256, 0, s>>>(n, b.st);
+    k_sort_prep<<<1, kSortBins, 0, s>>>(n, b.st);
     mark(2);
     nl += 3;
     const int64_t sort_tiles = (n + kSortTile - 1) / kSortTile;
     for (int pass = 0; pass < kSortPasses; ++pass) {
-        cudaMemsetAsync(b.lookback, 0, sizeof(uint32_t) * 256 * sort_tiles, s);
+        cudaMemsetAsync(b.lookback, 0, sizeof(uint32_t) * kSortBins * sort_tiles, s);
         k_onesweep<<<(unsigned)sort_tiles, kSortThreads, sizeof(SortSmem), s>>>(b.keys0, b.keys1, n, pass,
                                                                                  b.lookback, b.st, p.spin_limit,
                                                                                  p.stall_first_tile);

@@ -93,7 +93,7 @@ int ensure_build_capacity(se_ctx* c, int64_t n) {
     const int64_t scan_tiles = (cap + kScanTile - 1) / kScanTile;
     SE_CUDA(c, regrow(b.keys0, cap), "alloc keys");
     SE_CUDA(c, regrow(b.keys1, cap), "alloc keys");
-    SE_CUDA(c, regrow(b.lookback, sort_tiles * 256 + 64), "alloc lookback");
+    SE_CUDA(c, regrow(b.lookback, sort_tiles * kSortBins + 64), "alloc lookback");
     SE_CUDA(c, regrow(b.lookback64, scan_tiles + 64), "alloc lookback");
     SE_CUDA(c, regrow(b.codes, cap), "alloc codes");
     SE_CUDA(c, regrow(b.pts4, cap), "alloc points");

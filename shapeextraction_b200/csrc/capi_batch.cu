@@ -37,7 +37,7 @@ int lane_capacity(se_ctx* c, BatchLane& l, int64_t n) {
     const int64_t scan_tiles = (cap + kScanTile - 1) / kScanTile;
     SE_CUDA(c, regrow(b.keys0, cap), "alloc lane");
     SE_CUDA(c, regrow(b.keys1, cap), "alloc lane");
-    SE_CUDA(c, regrow(b.lookback, sort_tiles * 256 + 64), "alloc lane");
+    SE_CUDA(c, regrow(b.lookback, sort_tiles * kSortBins + 64), "alloc lane");
     SE_CUDA(c, regrow(b.lookback64, scan_tiles + 64), "alloc lane");
     SE_CUDA(c, regrow(b.codes, cap), "alloc lane");
     SE_CUDA(c, regrow(b.pts3, 3 * cap), "alloc lane");

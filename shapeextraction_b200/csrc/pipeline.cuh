@@ -8,6 +8,10 @@
 
 namespace shapex {
 
+// LSD radix sort of 64-bit keys in 9-bit digits: 7 passes cover the 63 bits of
+// a Morton code; the 8th (bit 63 alone) is trivial for codes and skipped.
+constexpr int kSortBits = 9;
+constexpr int kSortBins = 1 << kSortBits;
 constexpr int kSortPasses = 8;
 constexpr int kSortThreads = 512;
 constexpr int kSortIpt = 8;
@@ -35,8 +39,8 @@ struct DevState {
     int32_t pass_active[kSortPasses];
     int32_t pass_parity[kSortPasses];
     uint32_t tile_counter[16];              // dynamic tile ids: sort passes, dedup, octree scan
-    uint32_t hist[kSortPasses][256];        // per-digit histograms of the codes
-    uint32_t digit_off[kSortPasses][256];   // exclusive digit offsets
+    uint32_t hist[kSortPasses][kSortBins];       // per-digit histograms of the codes
+    uint32_t digit_off[kSortPasses][kSortBins];  // exclusive digit offsets
     unsigned long long u;                   // unique codes
     unsigned long long n_oct;               // octree nodes
     int32_t root_level;
@@ -159,7 +163,7 @@ cudaError_t enqueue_mlp_grad(const float* params, const float* X, const float* y
 cudaError_t enqueue_adam(float* params, const float* grads, float* m, float* v, float lr, int step, cudaStream_t s);
 
 // Sort n 64-bit keys in place in `keys` (ascending) with the onesweep passes;
-// `tmp` (n keys), `lookback` (256 words per 4096-key tile) and `st` are scratch.
+// `tmp` (n keys), `lookback` (kSortBins words per 4096-key tile) and `st` are scratch.
 cudaError_t enqueue_sort_keys(uint64_t* keys, uint64_t* tmp, int64_t n, uint32_t* lookback, DevState* st,
                               cudaStream_t s, int num_sms);
 

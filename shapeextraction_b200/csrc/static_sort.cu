@@ -11,7 +11,7 @@
 //
 // Scratch layout (one array, shared by every call on a device):
 //   [0, 8 MiB)       second key buffer for the ping-pong radix passes
-//   [8 MiB, +256 KiB) decoupled look-back words (256 per 4096-key tile)
+//   [8 MiB, +512 KiB) decoupled look-back words (512 per 4096-key tile)
 //   then              the sort's small device state (histograms, counters)
 
 #include <cstdint>
@@ -25,7 +25,7 @@ namespace {
 
 constexpr int64_t kMaxKeys = SE_STATIC_SORT_MAX_KEYS;
 constexpr size_t kKeyBytes = (size_t)kMaxKeys * sizeof(uint64_t);
-constexpr size_t kLookbackBytes = (size_t)((kMaxKeys + kSortTile - 1) / kSortTile) * 256 * sizeof(uint32_t);
+constexpr size_t kLookbackBytes = (size_t)((kMaxKeys + kSortTile - 1) / kSortTile) * kSortBins * sizeof(uint32_t);
 constexpr size_t kStateOffset = kKeyBytes + kLookbackBytes;
 constexpr size_t kScratchBytes = SE_STATIC_SORT_BYTES;
 static_assert(kKeyBytes % 256 == 0 && kLookbackBytes % 256 == 0, "scratch regions stay 256-byte aligned");
