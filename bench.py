@@ -491,7 +491,9 @@ def run_ours(a):
                 "d2h_bytes_per_step": int(12 * u),
                 "definition": "the same steps through the C ABI on two contexts and streams, driven by two host "
                               "threads (step i on context i mod 2): one step's input copy overlaps the other's "
-                              "build and search; CUDA events from before the first copy to the last normals"},
+                              "build and search; CUDA events from before the first copy to the last normals; no "
+                              f"L2 flush between steps: each step copies its input ({12 * n / 1e6:.0f} MB) in "
+                              "from the host" + (", more than the 126 MB L2" if 12 * n > 126e6 else "")},
             "roofline": roof,
             "step_roofline": step_roof,
             "pipeline": "learned-radius" if lrn is not None else "plain",
